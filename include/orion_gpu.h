@@ -1,0 +1,171 @@
+/*
+ * orion_gpu.h - C ABI of the B200 (sm_100a) implementation of ORION's per-step
+ * solver path.  Plain pointers and sizes only; no C++ or CUDA types cross it.
+ *
+ * Every function returns 0 on success and a negative ORION_E* code on error;
+ * orion_last_error() returns the message of the last failing call on the
+ * calling thread.  No exception crosses this boundary (the reference turns
+ * exceptions into std::exit(-1), src/solver/InviscidFluxComputer.cpp:534-540;
+ * here they become error codes).
+ *
+ * Data layout at the boundary is the reference's own: every per-block field is
+ * a padded array (idim+6) x (jdim+6) x (kdim+6) [x ncomp], i fastest, component
+ * slowest, exactly as OrionArray<double> stores it (src/core/OrionArray.hpp:240-261,
+ * src/preprocess/FlowField.cpp:73-85), so host<->device transfers are plain copies.
+ * Ghost layers: 3 (src/preprocess/FlowField.cpp:9-16).
+ */
+#ifndef ORION_GPU_H
+#define ORION_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORION_GPU_ABI_VERSION 1
+
+/* error codes */
+#define ORION_OK 0
+#define ORION_E_INVALID (-1)   /* bad argument */
+#define ORION_E_CUDA (-2)      /* CUDA runtime error */
+#define ORION_E_NOMEM (-3)     /* device allocation failed */
+#define ORION_E_UNSUPPORTED (-4)
+#define ORION_E_NUMERIC (-5)   /* non-finite residual */
+#define ORION_E_TIMEOUT (-6)   /* a bounded device wait gave up */
+
+/* precision of a case */
+#define ORION_PREC_FP64 0      /* plain form: every stage in FP64 */
+#define ORION_PREC_MIXED 1     /* FP32 flux/viscous/LU-SGS increments; FP64 metrics, Q update, norms */
+
+/* BC types (src/bc/PhysicalBC.cpp:576-613) */
+#define ORION_BC_INTERFACE (-1)
+#define ORION_BC_WALL 2
+#define ORION_BC_SYMMETRY 3
+#define ORION_BC_FARFIELD 4
+#define ORION_BC_FREESTREAM 5
+#define ORION_BC_EXTRAPOLATION 6
+
+/* fields of a block (names of src/preprocess/FlowField.hpp:19-71) */
+#define ORION_FIELD_PRIM 0     /* 6 comps: rho,u,v,w,p,T */
+#define ORION_FIELD_Q 1        /* 5 comps: conservative variables */
+#define ORION_FIELD_DQ 2       /* 5 comps: residual / increment */
+#define ORION_FIELD_METRICS 3  /* 9 comps: xi_x..zeta_z (times Jacobian) */
+#define ORION_FIELD_VOL 4      /* 1 comp */
+#define ORION_FIELD_DT 5       /* 1 comp: dt_phys / vol */
+#define ORION_FIELD_C 6        /* 1 comp: speed of sound */
+#define ORION_FIELD_MU 7       /* 1 comp: laminar viscosity */
+
+/* Flow parameters read by the hot path (subset of core::Params,
+ * src/core/Params.hpp:9-120, after init_inflow, src/preprocess/Inflow.cpp:300-459). */
+typedef struct {
+  double gamma;    /* inflow.gama */
+  double moo;      /* inflow.moo */
+  double reynolds; /* inflow.reynolds */
+  double prl;      /* inflow.prl */
+  double cfl;      /* step.cfl */
+  double twall;    /* inflow.twall (<= 1e-6: adiabatic wall) */
+  double tref;     /* inflow.tref */
+  double visc;     /* inflow.visc = 110.4 / tref (Sutherland constant) */
+  double roo, uoo, voo, woo, poo, too; /* non-dimensional freestream */
+  int nvis;        /* flowtype.nvis: 1 = Navier-Stokes */
+  int method;      /* control.method: 1 = finite difference */
+  int ntmst;       /* step.ntmst */
+  int csrv;        /* technic.csrv (an int in the reference) */
+} orion_params_t;
+
+/* One BC window (src/bc/BCData.hpp:8-54), 1-based inclusive point ranges. */
+typedef struct {
+  int s_st[3], s_ed[3];
+  int bctype;
+  int t_st[3], t_ed[3]; /* interfaces only */
+  int nbt;              /* interfaces only: target block, 1-based */
+  int ibcwin;           /* interfaces only: target region, 1-based */
+} orion_region_t;
+
+typedef struct {
+  int idim, jdim, kdim;           /* interior grid points */
+  int nregions;
+  const orion_region_t* regions;  /* in file order */
+} orion_block_desc_t;
+
+/* Residual statistics of one step (ResidualStats, src/solver/ResidualMonitor.hpp:8-12)
+ * plus the local physical time step (TimeIntegrator, params.step.phydtime). */
+typedef struct {
+  double rms;
+  double max;
+  int max_loc[5];   /* block (0-based), i, j, k (1-based interior), var (1-based) */
+  int pad;
+  double phydtime;
+} orion_residual_t;
+
+typedef struct orion_case_s* orion_case_t;
+
+const char* orion_last_error(void);
+int orion_abi_version(void);
+
+/* Device and case lifetime --------------------------------------------------
+ * Replaces the CUDA backend hook the reference's build expects
+ * (src/CMakeLists.txt:50-58 names backend/cuda/BackendCUDA.cu; the CPU hook is
+ * backend_cpu_init(), src/backend/cpu/BackendCPU.cpp:3-6). */
+int orion_gpu_init(int device);
+
+/* Creates a device-resident case: allocates every block's fields in one arena
+ * and builds the halo-copy, BC-phase and interface-averaging work lists from
+ * the region lists (the maps of src/bc/BCPreprocess.cpp:16-192). */
+int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion_params_t* params,
+                      int precision, orion_case_t* out);
+int orion_case_destroy(orion_case_t c);
+/* Optional: run on a caller-provided cudaStream_t (passed as void*); NULL = the case's own stream. */
+int orion_case_set_stream(orion_case_t c, void* stream);
+int orion_case_sync(orion_case_t c);
+/* Device bytes held by the case (the HBM footprint used for admission). */
+int orion_case_footprint(orion_case_t c, size_t* bytes);
+size_t orion_footprint_estimate(int nblocks, const orion_block_desc_t* blocks, int precision);
+
+/* Host <-> device copies of one block field (reference layout, FP64). */
+int orion_case_upload(orion_case_t c, int block, int field, const double* host);
+int orion_case_download(orion_case_t c, int block, int field, double* host);
+
+/* Set-up on the device: freestream + seeded noise on rho and u + EOS
+ * temperature (initialize_flow / update_temperature,
+ * src/preprocess/InitialCondition.cpp:7-147).  Noise: splitmix64(seed), draws
+ * 2n+1 and 2n+2 scale rho and u at padded point n (blocks in order, k,j,i). */
+int orion_case_init_flow(orion_case_t c, uint64_t seed, double amp);
+
+/* Grid metrics and Jacobian of one block on the host (compute_grid_metrics +
+ * check_grid_metrics, src/mesh/MetricComputer.cpp:103-500): x,y,z are
+ * idim*jdim*kdim, i fastest; metrics (9 comps) and vol are written in the
+ * padded layout, ghosts zero.  gcl=1 selects the Visbal conservative form. */
+int orion_grid_metrics_host(int idim, int jdim, int kdim, const double* x, const double* y,
+                            const double* z, int gcl, double* metrics, double* vol);
+
+/* Per-stage entry points, one per reference static method -------------------
+ * Each enqueues its kernels on the case stream and returns without waiting. */
+int orion_exchange_bc(orion_case_t c);                 /* HaloExchanger::exchange_bc, HaloExchanger.hpp:20-21 */
+int orion_apply_physical_bc(orion_case_t c);           /* bc::apply_physical_bc, PhysicalBC.hpp:17-19 */
+int orion_update_flow_states(orion_case_t c);          /* StateUpdater::update_flow_states, StateUpdater.hpp:14-15 */
+int orion_calculate_time_step(orion_case_t c);         /* TimeIntegrator::calculate_time_step, TimeIntegrator.hpp:10-11 */
+int orion_compute_viscous_rhs(orion_case_t c);         /* FluxComputer::compute_viscous_rhs, FluxComputer.hpp:15-16 */
+int orion_average_interface_residuals(orion_case_t c); /* HaloExchanger::average_interface_residuals, HaloExchanger.hpp:25 */
+int orion_compute_inviscid_rhs(orion_case_t c);        /* InviscidFluxComputer::compute_inviscid_rhs, InviscidFluxComputer.hpp:17-18 */
+int orion_update_solution(orion_case_t c);             /* StateUpdater::update_solution, StateUpdater.hpp:21-23 */
+int orion_residual_compute(orion_case_t c, orion_residual_t* out); /* ResidualMonitor::compute, ResidualMonitor.hpp:20-21 (waits) */
+int orion_phydtime(orion_case_t c, double* out);       /* params.step.phydtime after the last time step (waits) */
+
+/* Whole steps in the order of OrionSolver::solve (src/core/OrionSolver.cpp:141-209,
+ * without its debug block).  The step is captured once as a CUDA graph and
+ * replayed; residual statistics of every step go to a device history that is
+ * copied to `hist` (nsteps entries) when hist is not NULL.  Waits. */
+int orion_step(orion_case_t c, int nsteps, orion_residual_t* hist);
+/* Same, but enqueue only (no wait, no history copy); for overlapping cases. */
+int orion_step_async(orion_case_t c, int nsteps);
+/* Copies the residual of the most recent step (waits). */
+int orion_last_residual(orion_case_t c, orion_residual_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ORION_GPU_H */

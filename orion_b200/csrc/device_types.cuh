@@ -1,0 +1,92 @@
+// Device-side descriptors shared by the kernels and the host runtime.
+#pragma once
+#include <cstdint>
+
+namespace orion {
+
+constexpr int NG = 3;  // ghost layers (src/preprocess/FlowField.cpp:9-16)
+
+// One block's device arrays.  Every field is the reference's padded layout
+// (i fastest, component slowest, component stride npad).  S is the storage
+// type of the fields whose precision the mixed path lowers (dq, rhs, dt, c,
+// mu, coed, node derivatives); prim, q, metrics and vol are always FP64.
+template <typename S>
+struct BlockDev {
+  double* prim;           // 6 comps: rho,u,v,w,p,T
+  double* q;              // 5 comps
+  S* dq;                  // 5 comps
+  const double* metrics;  // 9 comps
+  const double* vol;
+  S* dt;
+  S* c;
+  S* mu;
+  S* rhs;                 // 5 comps, copy of the masked RHS for the sweeps
+  S* coed;                // LU-SGS diagonal coefficient
+  S* duvwt;               // 12 comps: node derivatives of u,v,w,T along xi,eta,zeta
+  const uint8_t* bcmask;  // 1 where a physical-BC window zeroes dq
+  int ni, nj, nk;         // interior points
+  int nx, ny, nz;         // padded
+  long long npad;
+  long long int_base;     // interior points of all earlier blocks (residual location key)
+};
+
+// Scalar parameters (orion_params_t after conversion).
+struct ParamsDev {
+  double gamma, moo, reynolds, prl, cfl, twall, tref, visc;
+  double roo, uoo, voo, woo, poo, too;
+  double csrv;
+  int nvis, method;
+};
+
+// A contiguous chunk of one block's points (padded or interior index space).
+struct Chunk {
+  int block;
+  int count;
+  long long start;
+};
+
+// A tile of whole grid lines of one block along one direction.
+struct LineTile {
+  int block;
+  int first;  // first line id (lines enumerate the two transverse interior coordinates)
+  int count;  // lines in the tile
+  int pad;
+};
+
+// One physical BC region, memory coordinates (ghost offset applied).
+struct RegionDev {
+  int block;
+  int type;
+  int dir;      // 0,1,2
+  int lr;       // +1 max face, otherwise min face
+  int s_nd;     // 1-based normal direction
+  int lo[3];    // inclusive window, memory coordinates
+  int hi[3];
+  int npts;
+  int is2d;     // symmetry in a k-thin block
+};
+
+// Wavefront plane work: for plane s of a block, jj,kk of the line set.
+struct PlaneChunk {
+  int block;
+  int start;  // first (jj + nj*kk) index
+  int count;
+  int pad;
+};
+
+// Residual partial of one CTA.
+struct ResPartial {
+  double sum;
+  double max;
+  long long key;  // lexicographic (block order, k, j, i, m) of the max
+};
+
+struct ResidualOut {
+  double rms;
+  double max;
+  int loc[5];
+  int pad;
+  double phydtime;
+};
+
+}  // namespace orion

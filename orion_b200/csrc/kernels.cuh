@@ -1,0 +1,1303 @@
+// Kernels of the per-step path.  Each kernel cites the reference routine whose
+// arithmetic it reproduces.  Templates: S = storage type of the lowered fields
+// (double for the plain form, float for the mixed form), T = compute type of
+// the flux / viscous / sweep arithmetic.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_types.cuh"
+#include "numerics.cuh"
+
+namespace orion {
+
+template <typename S>
+__device__ __forceinline__ long long lin(const BlockDev<S>& B, int i, int j, int k) {
+  return (long long)i + (long long)B.nx * ((long long)j + (long long)B.ny * (long long)k);
+}
+
+template <typename S>
+__device__ __forceinline__ int dim_along(const BlockDev<S>& B, int d) {
+  return d == 0 ? B.ni : (d == 1 ? B.nj : B.nk);
+}
+
+template <typename S>
+__device__ __forceinline__ long long stride_along(const BlockDev<S>& B, int d) {
+  return d == 0 ? 1LL : (d == 1 ? (long long)B.nx : (long long)B.nx * B.ny);
+}
+
+// Memory index of along-line coordinate 0 of line `l` in direction d.  Lines
+// enumerate the transverse interior coordinates, the lower one fastest.
+template <typename S>
+__device__ __forceinline__ long long line_origin(const BlockDev<S>& B, int d, int l) {
+  if (d == 0) {
+    const int jj = l % B.nj, kk = l / B.nj;
+    return lin(B, 0, NG + jj, NG + kk);
+  } else if (d == 1) {
+    const int ii = l % B.ni, kk = l / B.ni;
+    return lin(B, NG + ii, 0, NG + kk);
+  }
+  const int ii = l % B.ni, jj = l / B.ni;
+  return lin(B, NG + ii, NG + jj, 0);
+}
+
+// ===========================================================================
+// Halo copy of prim[0..4] into interface ghosts (HaloExchanger::exchange_bc,
+// src/solver/HaloExchanger.cpp:70-179).  The host flattened the pack/unpack
+// order into (src, dst) element offsets, last writer kept.
+// ===========================================================================
+__global__ void k_halo_copy(double* __restrict__ arena, const long long* __restrict__ src,
+                            const long long* __restrict__ dst, int n) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) arena[dst[t]] = arena[src[t]];
+}
+
+// ===========================================================================
+// Physical BCs (src/bc/PhysicalBC.cpp:12-613).  One launch per phase; phase p
+// holds the p-th physical region of every block (regions of one block are
+// sequential in file order; columns of one region are independent).
+// ===========================================================================
+template <typename S>
+__device__ __forceinline__ void bc_normal(const BlockDev<S>& B, long long idx, int s_nd, double& nx, double& ny,
+                                          double& nz) {
+  // get_normal (PhysicalBC.cpp:12-44)
+  const int off = (s_nd - 1) * 3;
+  const double mx = B.metrics[(off + 0) * B.npad + idx];
+  const double my = B.metrics[(off + 1) * B.npad + idx];
+  const double mz = B.metrics[(off + 2) * B.npad + idx];
+  double len = sqrt(mx * mx + my * my + mz * mz);
+  if (len < 1.0e-30) len = 1.0e-30;
+  nx = mx / len;
+  ny = my / len;
+  nz = mz / len;
+}
+
+template <typename S>
+__device__ __forceinline__ void dif_average(const BlockDev<S>& B, long long idx0, long long step_out) {
+  // apply_dif_average (PhysicalBC.cpp:71-92): face point = mean of ghost 1 and inner 1.
+  const long long ig = idx0 + step_out, ii = idx0 - step_out;
+  for (int m = 0; m < 6; ++m) {
+    const double vg = B.prim[m * B.npad + ig];
+    const double vi = B.prim[m * B.npad + ii];
+    B.prim[m * B.npad + idx0] = 0.5 * (vg + vi);
+  }
+}
+
+template <typename S>
+__global__ void k_bc_phase(const BlockDev<S>* __restrict__ blocks, const RegionDev* __restrict__ regions,
+                           const int* __restrict__ phase_regions, ParamsDev P) {
+  const RegionDev R = regions[phase_regions[blockIdx.y]];
+  const int pt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pt >= R.npts) return;
+  const BlockDev<S> B = blocks[R.block];
+  const int wi = R.hi[0] - R.lo[0] + 1, wj = R.hi[1] - R.lo[1] + 1;
+  const int i = R.lo[0] + pt % wi;
+  const int j = R.lo[1] + (pt / wi) % wj;
+  const int k = R.lo[2] + pt / (wi * wj);
+  const long long idx0 = lin(B, i, j, k);
+  const long long sd = (R.dir == 0) ? 1LL : (R.dir == 1 ? (long long)B.nx : (long long)B.nx * B.ny);
+  const long long out = (R.lr == 1) ? sd : -sd;  // step from the face towards the ghosts
+  const long long np = B.npad;
+  double* prim = B.prim;
+  auto PR = [&](int m, long long id) -> double& { return prim[m * np + id]; };
+
+  switch (R.type) {
+    case 2: {
+      if (P.nvis == 1) {
+        // apply_viscid_wall (PhysicalBC.cpp:254-363)
+        const double gama = P.gamma, mach = P.moo;
+        const double moocp = mach * mach * gama;
+        const bool isothermal = (P.twall > 1.0e-6);
+        const double twall_dim = (isothermal && fabs(P.tref) > 1e-16) ? P.twall / P.tref : P.twall;
+        const long long i1 = idx0 - out, i2 = idx0 - 2 * out;
+        const double p1 = PR(4, i1), p2 = PR(4, i2);
+        double p_wall = (4.0 * p1 - p2) / 3.0;
+        if (p_wall < 1.0e-6) p_wall = p1;
+        double t_wall;
+        if (isothermal) {
+          t_wall = twall_dim;
+        } else {
+          const double t1 = PR(5, i1), t2 = PR(5, i2);
+          t_wall = (4.0 * t1 - t2) / 3.0;
+          if (t_wall < 1e-6) t_wall = t1;
+        }
+        const double rho_wall = moocp * p_wall / t_wall;
+        for (int l = 0; l < NG; ++l) {
+          const int dist = l + 1;
+          const long long ig = idx0 + dist * out, ii = idx0 - dist * out;
+          const double u_i = PR(1, ii), v_i = PR(2, ii), w_i = PR(3, ii);
+          PR(1, ig) = -u_i;
+          PR(2, ig) = -v_i;
+          PR(3, ig) = -w_i;
+          PR(4, ig) = PR(4, ii);
+          if (isothermal) {
+            const double t_inner = PR(5, ii);
+            PR(5, ig) = 2.0 * t_wall - t_inner;
+          } else {
+            PR(5, ig) = PR(5, ii);
+          }
+          const double pg = PR(4, ig);
+          double tg = PR(5, ig);
+          if (tg < 1e-6) tg = 1.0;
+          const double rho_calc = moocp * pg / tg;
+          PR(0, ig) = (dist == 3) ? -rho_calc : rho_calc;
+        }
+        PR(0, idx0) = rho_wall;
+        PR(1, idx0) = 0.0;
+        PR(2, idx0) = 0.0;
+        PR(3, idx0) = 0.0;
+        PR(4, idx0) = p_wall;
+        PR(5, idx0) = t_wall;
+      } else {
+        // apply_inviscid_wall (PhysicalBC.cpp:191-248)
+        double nx, ny, nz;
+        bc_normal(B, idx0, R.s_nd, nx, ny, nz);
+        for (int l = 0; l < NG; ++l) {
+          const int dist = l + 1;
+          const long long ig = idx0 + dist * out, ii = idx0 - dist * out;
+          const double rho_i = PR(0, ii), u_i = PR(1, ii), v_i = PR(2, ii), w_i = PR(3, ii), p_i = PR(4, ii);
+          const double t_i = PR(5, ii);
+          const double v_dot_n = u_i * nx + v_i * ny + w_i * nz;
+          PR(0, ig) = (dist == 3) ? -rho_i : rho_i;
+          PR(1, ig) = u_i - 2.0 * v_dot_n * nx;
+          PR(2, ig) = v_i - 2.0 * v_dot_n * ny;
+          PR(3, ig) = w_i - 2.0 * v_dot_n * nz;
+          PR(4, ig) = p_i;
+          PR(5, ig) = t_i;
+        }
+        if (P.method == 1) dif_average(B, idx0, out);
+      }
+      break;
+    }
+    case 3: {
+      // apply_symmetry_bc (PhysicalBC.cpp:97-183)
+      if (R.is2d) {
+        for (int l = 0; l < NG; ++l) {
+          const int dist = l + 1;
+          const long long ig = idx0 + dist * out, ii = idx0 - dist * out;
+          PR(0, ig) = PR(0, ii);
+          PR(1, ig) = PR(1, ii);
+          PR(2, ig) = PR(2, ii);
+          PR(4, ig) = PR(4, ii);
+          PR(5, ig) = PR(5, ii);
+          PR(3, ig) = -PR(3, ii);
+        }
+      } else {
+        const int im = (R.lo[0] + R.hi[0]) / 2, jm = (R.lo[1] + R.hi[1]) / 2, km = (R.lo[2] + R.hi[2]) / 2;
+        double nx, ny, nz;
+        bc_normal(B, lin(B, im, jm, km), R.s_nd, nx, ny, nz);
+        for (int l = 0; l < NG; ++l) {
+          const int dist = l + 1;
+          const long long ig = idx0 + dist * out, ii = idx0 - dist * out;
+          const double rho = PR(0, ii), u = PR(1, ii), v = PR(2, ii), w = PR(3, ii), p = PR(4, ii);
+          const double v_dot_n = u * nx + v * ny + w * nz;
+          PR(0, ig) = rho;
+          PR(1, ig) = u - 2.0 * v_dot_n * nx;
+          PR(2, ig) = v - 2.0 * v_dot_n * ny;
+          PR(3, ig) = w - 2.0 * v_dot_n * nz;
+          PR(4, ig) = p;
+          PR(5, ig) = PR(5, ii);
+        }
+      }
+      if (P.method == 1) dif_average(B, idx0, out);
+      break;
+    }
+    case 4: {
+      // apply_farfield_bc (PhysicalBC.cpp:369-472)
+      const double gama = P.gamma, gm1 = gama - 1.0;
+      const double rho_inf = P.roo, u_inf = P.uoo, v_inf = P.voo, w_inf = P.woo, p_inf = P.poo;
+      const double c_inf = sqrt(gama * p_inf / rho_inf);
+      double nx, ny, nz;
+      bc_normal(B, idx0, R.s_nd, nx, ny, nz);
+      if (R.lr == -1) {
+        nx = -nx;
+        ny = -ny;
+        nz = -nz;
+      }
+      const long long ii = idx0 - out;
+      const double rho_in = PR(0, ii), u_in = PR(1, ii), v_in = PR(2, ii), w_in = PR(3, ii), p_in = PR(4, ii);
+      const double c_in = sqrt(gama * p_in / rho_in);
+      const double s_in = p_in / pow(rho_in, gama);
+      const double s_inf = p_inf / pow(rho_inf, gama);
+      const double vn_in = u_in * nx + v_in * ny + w_in * nz;
+      const double vn_inf = u_inf * nx + v_inf * ny + w_inf * nz;
+      const double vel_mag = sqrt(u_in * u_in + v_in * v_in + w_in * w_in);
+      const double mach = vel_mag / c_in;
+      double rho_b, u_b, v_b, w_b, p_b;
+      if (mach < 1.0) {
+        const double R_plus = vn_in + 2.0 * c_in / gm1;
+        const double R_minus = vn_inf - 2.0 * c_inf / gm1;
+        const double vn_b = 0.5 * (R_plus + R_minus);
+        const double c_b = 0.25 * gm1 * (R_plus - R_minus);
+        double s_b, u_ref, v_ref, w_ref, vn_ref;
+        if (vn_b > 0.0) {
+          s_b = s_in; u_ref = u_in; v_ref = v_in; w_ref = w_in; vn_ref = vn_in;
+        } else {
+          s_b = s_inf; u_ref = u_inf; v_ref = v_inf; w_ref = w_inf; vn_ref = vn_inf;
+        }
+        rho_b = pow(c_b * c_b / (gama * s_b), 1.0 / gm1);
+        p_b = s_b * pow(rho_b, gama);
+        u_b = u_ref + (vn_b - vn_ref) * nx;
+        v_b = v_ref + (vn_b - vn_ref) * ny;
+        w_b = w_ref + (vn_b - vn_ref) * nz;
+      } else {
+        if (vn_in > 0.0) {
+          rho_b = rho_in; u_b = u_in; v_b = v_in; w_b = w_in; p_b = p_in;
+        } else {
+          rho_b = rho_inf; u_b = u_inf; v_b = v_inf; w_b = w_inf; p_b = p_inf;
+        }
+      }
+      const double t_b = (mach * mach * gama) * p_b / rho_b;
+      for (int l = 0; l < NG; ++l) {
+        const int dist = l + 1;
+        const long long ig = idx0 + dist * out;
+        PR(0, ig) = (dist == 3) ? -rho_b : rho_b;
+        PR(1, ig) = u_b;
+        PR(2, ig) = v_b;
+        PR(3, ig) = w_b;
+        PR(4, ig) = p_b;
+        PR(5, ig) = t_b;
+      }
+      break;
+    }
+    case 5: {
+      // apply_freestream_bc (PhysicalBC.cpp:477-521)
+      for (int l = 0; l < NG; ++l) {
+        const long long ig = idx0 + (l + 1) * out;
+        PR(0, ig) = P.roo;
+        PR(1, ig) = P.uoo;
+        PR(2, ig) = P.voo;
+        PR(3, ig) = P.woo;
+        PR(4, ig) = P.poo;
+        PR(5, ig) = P.too;
+      }
+      break;
+    }
+    case 6: {
+      // apply_extrapolation_bc (PhysicalBC.cpp:526-571)
+      const long long is = idx0 - out;
+      double v[6];
+      for (int m = 0; m < 6; ++m) v[m] = PR(m, is);
+      for (int l = 0; l < NG; ++l) {
+        const long long ig = idx0 + (l + 1) * out;
+        for (int m = 0; m < 6; ++m) PR(m, ig) = v[m];
+      }
+      break;
+    }
+    default:
+      break;
+  }
+}
+
+// ===========================================================================
+// Derived state + dq := 0 (+ local time step when DO_DT)
+// update_flow_states (src/solver/StateUpdater.cpp:15-168) and
+// calculate_spectrum / calculate_local_dt_cell (src/solver/TimeIntegrator.cpp:20-125),
+// one pass over the padded points.  The spectral radii are consumed in place
+// (they are read nowhere else).  phydtime = min(1000, min dt*vol) via atomicMin
+// on the bit pattern of a positive double.
+// ===========================================================================
+template <typename S, bool DO_Q>
+__device__ __forceinline__ void state_point(const BlockDev<S>& B, const ParamsDev& P, long long idx, int i, int j,
+                                            int k, double& c_out, double& mu_out) {
+  const long long np = B.npad;
+  const bool inI = (i >= NG && i < NG + B.ni), inJ = (j >= NG && j < NG + B.nj), inK = (k >= NG && k < NG + B.nk);
+  const int nin = (int)inI + (int)inJ + (int)inK;
+  double* prim = B.prim;
+  double T = prim[5 * np + idx];
+  double cval = (double)B.c[idx];
+  if (nin >= 2) {
+    // interior (nin == 3) or ghost face slab (nin == 2), update_thermodynamics_block
+    double rho = prim[idx];
+    const double p = prim[4 * np + idx];
+    if (nin == 2) rho = fabs(rho);
+    const double a2 = P.gamma * p / rho;
+    cval = sqrt(fabs(a2));
+    B.c[idx] = (S)cval;
+    if (P.nvis == 1) {
+      T = (P.moo * P.moo) * a2;
+      prim[5 * np + idx] = T;
+    }
+    if (DO_Q) {
+      // update_conservative_block (StateUpdater.cpp:94-149)
+      const double r0 = prim[idx], u = prim[np + idx], v = prim[2 * np + idx], w = prim[3 * np + idx];
+      const bool use_abs = (nin == 2);
+      const double rc = (use_abs || r0 < 0.0) ? fabs(r0) : r0;
+      const double gm1_inv = 1.0 / (P.gamma - 1.0);
+      B.q[idx] = rc;
+      B.q[np + idx] = rc * u;
+      B.q[2 * np + idx] = rc * v;
+      B.q[3 * np + idx] = rc * w;
+      const double ke = 0.5 * rc * (u * u + v * v + w * w);
+      B.q[4 * np + idx] = p * gm1_inv + ke;
+    }
+  }
+  double muv = (double)B.mu[idx];
+  if (P.nvis == 1) {
+    // update_viscosity_block (StateUpdater.cpp:75-92): whole padded array
+    double tm = T;
+    if (tm < 1e-6) tm = 1e-6;
+    muv = tm * sqrt(tm) * (1.0 + P.visc) / (tm + P.visc);
+    B.mu[idx] = (S)muv;
+  }
+  for (int m = 0; m < 5; ++m) B.dq[m * np + idx] = (S)0;
+  c_out = cval;
+  mu_out = muv;
+}
+
+template <typename S>
+__device__ __forceinline__ double timestep_point(const BlockDev<S>& B, const ParamsDev& P, long long idx, double c,
+                                                 double mu) {
+  // calculate_spectrum + calculate_local_dt_cell (TimeIntegrator.cpp:20-125)
+  const long long np = B.npad;
+  const double u = B.prim[np + idx], v = B.prim[2 * np + idx], w = B.prim[3 * np + idx];
+  const double rho = B.prim[idx];
+  const double vol = B.vol[idx];
+  double sum_spec = 0.0;
+  for (int d = 0; d < 3; ++d) {
+    const double mx = B.metrics[(3 * d + 0) * np + idx];
+    const double my = B.metrics[(3 * d + 1) * np + idx];
+    const double mz = B.metrics[(3 * d + 2) * np + idx];
+    const double U_contra = fabs(u * mx + v * my + w * mz);
+    const double grad_len = sqrt(mx * mx + my * my + mz * mz);
+    const double spec = U_contra + c * grad_len;
+    double specv = 0.0;
+    if (P.nvis == 1) {
+      const double grad_sq = mx * mx + my * my + mz * mz;
+      const double denom = P.reynolds * rho * vol + 1.0e-30;
+      specv = (2.0 * mu / denom) * grad_sq * P.csrv;
+    }
+    sum_spec += spec + specv;
+  }
+  const double dt_phys = P.cfl / (sum_spec + 1.0e-30);
+  return dt_phys / vol;
+}
+
+__device__ __forceinline__ void atomic_min_pos_double(unsigned long long* addr, double v) {
+  // positive doubles order like their bit patterns
+  if (v >= 0.0) atomicMin(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+template <typename S, bool DO_Q, bool DO_DT>
+__global__ void k_state(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P,
+                        unsigned long long* __restrict__ dtmin_bits) {
+  const Chunk ch = chunks[blockIdx.x];
+  const BlockDev<S> B = blocks[ch.block];
+  double local_min = 1000.0;
+  for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+    const long long idx = ch.start + t;
+    const int i = (int)(idx % B.nx);
+    const int j = (int)((idx / B.nx) % B.ny);
+    const int k = (int)(idx / ((long long)B.nx * B.ny));
+    double c, mu;
+    state_point<S, DO_Q>(B, P, idx, i, j, k, c, mu);
+    if (DO_DT) {
+      const bool interior = (i >= NG && i < NG + B.ni && j >= NG && j < NG + B.nj && k >= NG && k < NG + B.nk);
+      if (interior) {
+        const double dtv = timestep_point(B, P, idx, c, mu);
+        B.dt[idx] = (S)dtv;
+        const double dt_phys = (double)(S)dtv * B.vol[idx];
+        if (dt_phys < local_min) local_min = dt_phys;
+      }
+    }
+  }
+  if (DO_DT) atomic_min_pos_double(dtmin_bits, local_min);
+}
+
+// time step alone (per-stage entry point): interior points of interior chunks
+template <typename S>
+__global__ void k_timestep(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P,
+                           unsigned long long* __restrict__ dtmin_bits) {
+  const Chunk ch = chunks[blockIdx.x];
+  const BlockDev<S> B = blocks[ch.block];
+  double local_min = 1000.0;
+  for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+    const long long n = ch.start + t;  // interior index
+    const int ii = (int)(n % B.ni), jj = (int)((n / B.ni) % B.nj), kk = (int)(n / ((long long)B.ni * B.nj));
+    const long long idx = lin(B, NG + ii, NG + jj, NG + kk);
+    const double dtv = timestep_point(B, P, idx, (double)B.c[idx], (double)B.mu[idx]);
+    B.dt[idx] = (S)dtv;
+    const double dt_phys = (double)(S)dtv * B.vol[idx];
+    if (dt_phys < local_min) local_min = dt_phys;
+  }
+  atomic_min_pos_double(dtmin_bits, local_min);
+}
+
+__global__ void k_step_begin(unsigned long long* dtmin_bits) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *dtmin_bits = (unsigned long long)__double_as_longlong(1000.0);
+}
+
+// ===========================================================================
+// Node derivatives of (u,v,w,T) along xi, eta, zeta at interior points
+// (compute_derivatives_cell + compute_node_deriv_line,
+// src/solver/FluxComputer.cpp:13-67, 301-376).
+// ===========================================================================
+template <typename T>
+__device__ __forceinline__ T node_deriv(const double* __restrict__ q, long long o, long long st, int t, int L,
+                                        bool fl, bool fr) {
+  // q + o is memory coordinate 0 of the line, st the along-line stride, t the interior index.
+  auto Q = [&](int p) -> T { return (T)q[o + (long long)p * st]; };
+  if (fl && t == 0) {
+    const T q1 = Q(3), q2 = Q(4), q3 = Q(5), q4 = Q(6);
+    return (T(-11) * q1 + T(18) * q2 - T(9) * q3 + T(2) * q4) / T(6);
+  }
+  if (fl && t == 1) {
+    const T q1 = Q(3), q2 = Q(4), q3 = Q(5), q4 = Q(6), q5 = Q(7);
+    return (T(-3) * q1 + T(-10) * q2 + T(18) * q3 + T(-6) * q4 + T(1) * q5) / T(12);
+  }
+  if (fr && t == L - 1) {
+    const T qn = Q(L + 2), qn_1 = Q(L + 1), qn_2 = Q(L), qn_3 = Q(L - 1);
+    return -(T(-11) * qn + T(18) * qn_1 - T(9) * qn_2 + T(2) * qn_3) / T(6);
+  }
+  if (fr && t == L - 2) {
+    const T qn = Q(L + 2), qn_1 = Q(L + 1), qn_2 = Q(L), qn_3 = Q(L - 1), qn_4 = Q(L - 2);
+    return -(T(-3) * qn + T(-10) * qn_1 + T(18) * qn_2 + T(-6) * qn_3 + T(1) * qn_4) / T(12);
+  }
+  const int p = t + NG;
+  return (T(8) * (Q(p + 1) - Q(p - 1)) + T(-1) * (Q(p + 2) - Q(p - 2))) / T(12);
+}
+
+template <typename S, typename T>
+__global__ void k_node_derivs(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks) {
+  const Chunk ch = chunks[blockIdx.x];
+  const BlockDev<S> B = blocks[ch.block];
+  const long long np = B.npad;
+  for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+    const long long n = ch.start + t;
+    const int ii = (int)(n % B.ni), jj = (int)((n / B.ni) % B.nj), kk = (int)(n / ((long long)B.ni * B.nj));
+    const long long idx = lin(B, NG + ii, NG + jj, NG + kk);
+    const int tt[3] = {ii, jj, kk};
+    for (int d = 0; d < 3; ++d) {
+      const long long st = stride_along(B, d);
+      const long long o = idx - (long long)(tt[d] + NG) * st;  // along-line coordinate 0
+      const int L = dim_along(B, d);
+      const bool fl = B.prim[o] < 0.0;
+      const bool fr = B.prim[o + (long long)(L + 5) * st] < 0.0;
+      const int comp[4] = {1, 2, 3, 5};
+      for (int m = 0; m < 4; ++m) {
+        const T v = node_deriv<T>(B.prim + comp[m] * np, o, st, tt[d], L, fl, fr);
+        B.duvwt[(m + 4 * d) * np + idx] = (S)v;
+      }
+    }
+  }
+}
+
+// ===========================================================================
+// Viscous RHS along one direction D (compute_viscous_flux_block,
+// src/solver/FluxComputer.cpp:466-722, with interp_line_to_half :129-178,
+// compute_half_deriv_line :72-124, transform_derivs_to_phys :183-205,
+// compute_viscous_flux_1d :210-252, compute_flux_diff_1d :257-296).
+// One CTA per tile of whole lines: face fluxes to shared memory, then the
+// 6th-order difference and dq -= dfv / Re.
+// ===========================================================================
+template <typename T>
+__device__ __forceinline__ T interp_half(const double* __restrict__ a, long long o, long long st, int f, int L,
+                                         bool fl, bool fr) {
+  // interp_line_to_half at face f of a line of L points; a + o is memory coordinate 0.
+  auto Q = [&](int p) -> T { return (T)a[o + (long long)p * st]; };
+  if (fl && f == 0) return (T(35) * Q(3) + T(-35) * Q(4) + T(21) * Q(5) + T(-5) * Q(6)) / T(16);
+  if (fl && f == 1) return (T(5) * Q(3) + T(15) * Q(4) + T(-5) * Q(5) + T(1) * Q(6)) / T(16);
+  if (fr && f == L) return (T(35) * Q(L + 2) + T(-35) * Q(L + 1) + T(21) * Q(L) + T(-5) * Q(L - 1)) / T(16);
+  if (fr && f == L - 1) return (T(5) * Q(L + 2) + T(15) * Q(L + 1) + T(-5) * Q(L) + T(1) * Q(L - 1)) / T(16);
+  return (T(9) * (Q(f + 2) + Q(f + 3)) + T(-1) * (Q(f + 4) + Q(f + 1))) / T(16);
+}
+
+template <typename T, typename S>
+__device__ __forceinline__ T interp_half_s(const S* __restrict__ a, long long o, long long st, int f) {
+  auto Q = [&](int p) -> T { return (T)a[o + (long long)p * st]; };
+  return (T(9) * (Q(f + 2) + Q(f + 3)) + T(-1) * (Q(f + 4) + Q(f + 1))) / T(16);
+}
+
+template <typename T>
+__device__ __forceinline__ T half_deriv(const double* __restrict__ a, long long o, long long st, int f, int L, bool fl,
+                                        bool fr) {
+  auto Q = [&](int p) -> T { return (T)a[o + (long long)p * st]; };
+  if (fl && f == 0) return (T(-71) * Q(3) + T(141) * Q(4) + T(-93) * Q(5) + T(23) * Q(6)) / T(24);
+  if (fl && f == 1) return (T(-22) * Q(3) + T(17) * Q(4) + T(9) * Q(5) + T(-5) * Q(6) + T(1) * Q(7)) / T(24);
+  if (fr && f == L) return -(T(-71) * Q(L + 2) + T(141) * Q(L + 1) + T(-93) * Q(L) + T(23) * Q(L - 1)) / T(24);
+  if (fr && f == L - 1)
+    return -(T(-22) * Q(L + 2) + T(17) * Q(L + 1) + T(9) * Q(L) + T(-5) * Q(L - 1) + T(1) * Q(L - 2)) / T(24);
+  return (T(27) * (Q(f + 3) - Q(f + 2)) + T(-1) * (Q(f + 4) - Q(f + 1))) / T(24);
+}
+
+// cross derivative interpolated to face f with the source index clamped to the interior
+template <typename T, typename S>
+__device__ __forceinline__ T cross_half(const S* __restrict__ a, long long o, long long st, int f, int L) {
+  auto Q = [&](int p) -> T {
+    const int pc = p < NG ? NG : (p > L + NG - 1 ? L + NG - 1 : p);
+    return (T)a[o + (long long)pc * st];
+  };
+  return (T(9) * (Q(f + 2) + Q(f + 3)) + T(-1) * (Q(f + 4) + Q(f + 1))) / T(16);
+}
+
+template <int D, typename S, typename T>
+__device__ __forceinline__ void viscous_face(const BlockDev<S>& B, const ParamsDev& P, long long o, int f, int L,
+                                             bool fl, bool fr, T cp_prl, T fv[4]) {
+  const long long np = B.npad;
+  const long long st = stride_along(B, D);
+  const double* prim = B.prim;
+  T uvwt[4];
+  const int comp[4] = {1, 2, 3, 5};
+  for (int m = 0; m < 4; ++m) uvwt[m] = interp_half<T>(prim + comp[m] * np, o, st, f, L, fl, fr);
+  const T vs = interp_half_s<T, S>(B.mu, o, st, f);
+  const T kcp = vs * cp_prl;
+  const T volh = interp_half_s<T, double>(B.vol, o, st, f);
+  T kxyz[9];
+  for (int m = 0; m < 9; ++m) kxyz[m] = interp_half_s<T, double>(B.metrics + m * np, o, st, f);
+  T d[12];
+  // derivative along the line (half point), cross derivatives interpolated
+  for (int m = 0; m < 4; ++m) d[m + 4 * D] = half_deriv<T>(prim + comp[m] * np, o, st, f, L, fl, fr);
+#pragma unroll
+  for (int dd = 0; dd < 3; ++dd) {
+    if (dd == D) continue;
+    for (int m = 0; m < 4; ++m) d[m + 4 * dd] = cross_half<T, S>(B.duvwt + (m + 4 * dd) * np, o, st, f, L);
+  }
+  // transform_derivs_to_phys
+  const T vol_inv = T(1) / volh;
+  T g[12];
+  for (int m = 0; m < 3; ++m) {
+    const T k1 = kxyz[m], k2 = kxyz[m + 3], k3 = kxyz[m + 6];
+    for (int v = 0; v < 4; ++v) g[v * 3 + m] = (k1 * d[v] + k2 * d[v + 4] + k3 * d[v + 8]) * vol_inv;
+  }
+  // compute_viscous_flux_1d
+  const T CC = T(2.0 / 3.0);
+  const T vscc = vs * CC;
+  const T dudx = g[0], dudy = g[1], dudz = g[2];
+  const T dvdx = g[3], dvdy = g[4], dvdz = g[5];
+  const T dwdx = g[6], dwdy = g[7], dwdz = g[8];
+  const T txx = vscc * (T(2) * dudx - dvdy - dwdz);
+  const T tyy = vscc * (T(2) * dvdy - dwdz - dudx);
+  const T tzz = vscc * (T(2) * dwdz - dudx - dvdy);
+  const T txy = vs * (dudy + dvdx);
+  const T txz = vs * (dudz + dwdx);
+  const T tyz = vs * (dvdz + dwdy);
+  const T nx = kxyz[3 * D + 0], ny = kxyz[3 * D + 1], nz = kxyz[3 * D + 2];
+  fv[0] = txx * nx + txy * ny + txz * nz;
+  fv[1] = txy * nx + tyy * ny + tyz * nz;
+  fv[2] = txz * nx + tyz * ny + tzz * nz;
+  const T work = uvwt[0] * fv[0] + uvwt[1] * fv[1] + uvwt[2] * fv[2];
+  const T heat = kcp * (g[9] * nx + g[10] * ny + g[11] * nz);
+  fv[3] = work + heat;
+}
+
+template <int D>
+__device__ __forceinline__ void tile_item(int it, int nlanes, int nfaces, int& lane, int& pos) {
+  if (D == 0) {
+    lane = it / nfaces;
+    pos = it - lane * nfaces;
+  } else {
+    pos = it / nlanes;
+    lane = it - pos * nlanes;
+  }
+}
+
+template <int D, typename S, typename T>
+__global__ void k_viscous(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles, ParamsDev P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* fsh = reinterpret_cast<T*>(smem_raw);
+  const LineTile tl = tiles[blockIdx.x];
+  const BlockDev<S> B = blocks[tl.block];
+  const int L = dim_along(B, D);
+  const int nf = L + 1;
+  const long long st = stride_along(B, D);
+  const T cp = T(1) / ((T(P.gamma) - T(1)) * T(P.moo) * T(P.moo));
+  const T cp_prl = cp / T(P.prl);
+  const T re_inv = (fabs(P.reynolds) > 1.0e-30) ? T(1) / T(P.reynolds) : T(0);
+  const int nitems = tl.count * nf;
+  for (int it = threadIdx.x; it < nitems; it += blockDim.x) {
+    int lane, f;
+    tile_item<D>(it, tl.count, nf, lane, f);
+    const long long o = line_origin(B, D, tl.first + lane);
+    const bool fl = B.prim[o] < 0.0;
+    const bool fr = B.prim[o + (long long)(L + 5) * st] < 0.0;
+    T fv[4];
+    viscous_face<D, S, T>(B, P, o, f, L, fl, fr, cp_prl, fv);
+    T* dst = fsh + ((size_t)lane * nf + f) * 4;
+    dst[0] = fv[0];
+    dst[1] = fv[1];
+    dst[2] = fv[2];
+    dst[3] = fv[3];
+  }
+  __syncthreads();
+  const int npts = tl.count * L;
+  for (int it = threadIdx.x; it < npts; it += blockDim.x) {
+    int lane, t;
+    tile_item<D>(it, tl.count, L, lane, t);
+    const long long o = line_origin(B, D, tl.first + lane);
+    const long long idx = o + (long long)(t + NG) * st;
+    const T* fb = fsh + (size_t)lane * nf * 4;
+    for (int m = 0; m < 4; ++m) {
+      const T dfv = flux_diff<T>(fb + m, 4, t, L);
+      S* q = B.dq + (m + 1) * B.npad + idx;
+      *q = (S)((T)*q - re_inv * dfv);
+    }
+  }
+}
+
+// ===========================================================================
+// Inviscid RHS along one direction D (compute_block_inviscid + compute_flux_line,
+// src/solver/InviscidFluxComputer.cpp:136-192, 238-522, 543-647).
+// Face fluxes from WCNS-E-5 states (fixed stencils where the ghost-3 density
+// flag is set) and the Roe flux, then the flux difference; the boundary
+// re-calculation rounds (:377-521) are evaluated per output point by the
+// threads of points 0..2 and L-3..L-1 of flagged line ends.
+// ===========================================================================
+template <typename S, typename T>
+struct InvLine {
+  const double* prim;
+  long long o, st, np;
+  int L;
+  __device__ __forceinline__ T q(int p, int m) const { return (T)prim[m * np + o + (long long)p * st]; }
+};
+
+template <typename S, typename T>
+__device__ __forceinline__ T metric_half(const BlockDev<S>& B, int mc, long long o, long long st, int f, int L) {
+  // interp_metrics_half (InviscidFluxComputer.cpp:136-192), ni > 2
+  const double* a = B.metrics + mc * B.npad;
+  auto Q = [&](int p) -> T { return (T)a[o + (long long)p * st]; };
+  if (f == 0) return (T(35) * Q(3) + T(-35) * Q(4) + T(21) * Q(5) + T(-5) * Q(6)) / T(16);
+  if (f == 1) return (T(5) * Q(3) + T(15) * Q(4) + T(-5) * Q(5) + T(1) * Q(6)) / T(16);
+  if (f == L) return (T(35) * Q(L + 2) + T(-35) * Q(L + 1) + T(21) * Q(L) + T(-5) * Q(L - 1)) / T(16);
+  if (f == L - 1) return (T(5) * Q(L + 2) + T(15) * Q(L + 1) + T(-5) * Q(L) + T(1) * Q(L - 1)) / T(16);
+  return (T(9) * (Q(f + 2) + Q(f + 3)) + T(-1) * (Q(f + 4) + Q(f + 1))) / T(16);
+}
+
+// Initial left/right states at face f (main WCNS loop + fixed boundary stencils).
+template <typename S, typename T>
+__device__ __forceinline__ void initial_states(const InvLine<S, T>& ln, int f, bool fl, bool fr, T ql[5], T qr[5]) {
+  const int L = ln.L;
+  const int ist = fl ? 2 : 0, ied = fr ? L - 2 : L;
+  for (int m = 0; m < 5; ++m) {
+    T l = T(0), r = T(0);
+    if (f >= ist && f <= ied) {
+      const T a0 = ln.q(f, m), a1 = ln.q(f + 1, m), a2 = ln.q(f + 2, m), a3 = ln.q(f + 3, m), a4 = ln.q(f + 4, m),
+              a5 = ln.q(f + 5, m);
+      l = wcns_left<T>(a0, a1, a2, a3, a4);
+      r = wcns_right<T>(a1, a2, a3, a4, a5);
+    }
+    if (ist > 1 && f <= 2) {
+      const T q1 = ln.q(3, m), q2 = ln.q(4, m), q3 = ln.q(5, m), q4 = ln.q(6, m);
+      if (f == 0) {
+        l = (T(35.) * q1 - T(35.) * q2 + T(21.) * q3 - T(5.) * q4) / T(16.);
+        r = l;
+      } else if (f == 1) {
+        l = (T(5.) * q1 + T(15.) * q2 - T(5.) * q3 + q4) / T(16.);
+        r = l;
+      } else {
+        l = (-q1 + T(9.) * q2 + T(9.) * q3 - q4) / T(16.);
+      }
+    }
+    if (ied < L && f >= L - 2) {
+      const T qn = ln.q(L + 2, m), qn1 = ln.q(L + 1, m), qn2 = ln.q(L, m), qn3 = ln.q(L - 1, m);
+      if (f == L) {
+        r = (T(35.) * qn - T(35.) * qn1 + T(21.) * qn2 - T(5.) * qn3) / T(16.);
+        l = r;
+      } else if (f == L - 1) {
+        r = (T(5.) * qn + T(15.) * qn1 - T(5.) * qn2 + qn3) / T(16.);
+        l = r;
+      } else {
+        r = (-qn + T(9.) * qn1 + T(9.) * qn2 - qn3) / T(16.);
+      }
+    }
+    ql[m] = l;
+    qr[m] = r;
+  }
+}
+
+template <int D, typename S, typename T>
+__device__ __forceinline__ void face_metric(const BlockDev<S>& B, long long o, long long st, int f, int L, T& kx,
+                                            T& ky, T& kz) {
+  kx = metric_half<S, T>(B, 3 * D + 0, o, st, f, L);
+  ky = metric_half<S, T>(B, 3 * D + 1, o, st, f, L);
+  kz = metric_half<S, T>(B, 3 * D + 2, o, st, f, L);
+}
+
+// Positivity fallback + Roe flux at face f (calc_flux_loop, InviscidFluxComputer.cpp:342-364).
+template <typename S, typename T>
+__device__ __forceinline__ void fallback_roe(const InvLine<S, T>& ln, int f, T ql[5], T qr[5], T kx, T ky, T kz,
+                                             T gamma, T out[5]) {
+  const int L = ln.L;
+  if (ql[0] <= T(1e-6) || ql[4] <= T(1e-6)) {
+    const int p = (f - 1 > 0 ? f - 1 : 0) + 2;
+    for (int m = 0; m < 5; ++m) ql[m] = ln.q(p, m);
+  }
+  if (qr[0] <= T(1e-6) || qr[4] <= T(1e-6)) {
+    const int p = (L - 1 < f ? L - 1 : f) + 3;
+    for (int m = 0; m < 5; ++m) qr[m] = ln.q(p, m);
+  }
+  roe_flux<T>(ql, qr, kx, ky, kz, T(0), T(0.1), gamma, out);
+}
+
+// Left-end re-calculation rounds (InviscidFluxComputer.cpp:377-448): the value
+// of fc[t] for t = 0, 1, 2 when the ghost-3 density flag is set.
+template <int D, typename S, typename T>
+__device__ void cascade_left(const BlockDev<S>& B, const InvLine<S, T>& ln, int t, T gamma, T fc[5]) {
+  T F[6][5];
+  auto flux_eq = [&](int f, const T s[5]) {
+    T ql[5], qr[5];
+    for (int m = 0; m < 5; ++m) { ql[m] = s[m]; qr[m] = s[m]; }
+    T kx, ky, kz;
+    face_metric<D, S, T>(B, ln.o, ln.st, f, ln.L, kx, ky, kz);
+    fallback_roe<S, T>(ln, f, ql, qr, kx, ky, kz, gamma, F[f]);
+  };
+  auto flux_lr = [&](int f, const T l[5], const T r[5]) {
+    T ql[5], qr[5];
+    for (int m = 0; m < 5; ++m) { ql[m] = l[m]; qr[m] = r[m]; }
+    T kx, ky, kz;
+    face_metric<D, S, T>(B, ln.o, ln.st, f, ln.L, kx, ky, kz);
+    fallback_roe<S, T>(ln, f, ql, qr, kx, ky, kz, gamma, F[f]);
+  };
+  T Q3[5], Q4[5], Q5[5], Q6[5];
+  for (int m = 0; m < 5; ++m) { Q3[m] = ln.q(3, m); Q4[m] = ln.q(4, m); Q5[m] = ln.q(5, m); Q6[m] = ln.q(6, m); }
+  T s[5], s2[5];
+  if (t == 0) {
+    for (int m = 0; m < 5; ++m) s[m] = (T(3.) * Q3[m] - T(1.) * Q4[m]) / T(2.0);
+    flux_eq(0, s);
+    for (int m = 0; m < 5; ++m) s[m] = (T(19.) * Q3[m] + T(25.) * Q4[m] - T(2.) * Q5[m]) / T(42.0);
+    flux_eq(1, s);
+    for (int m = 0; m < 5; ++m) s[m] = (T(4.) * Q3[m] + T(3.) * Q4[m] + T(9.) * Q5[m] + T(2.) * Q6[m]) / T(18.0);
+    flux_eq(2, s);
+    for (int m = 0; m < 5; ++m) s[m] = (T(-2.) * Q3[m] + T(3.) * Q4[m] + T(3.) * Q5[m] + T(2.) * Q6[m]) / T(6.0);
+    flux_eq(3, s);
+    for (int m = 0; m < 5; ++m) fc[m] = (T(-23.) * F[0][m] + T(21.) * F[1][m] + T(3.) * F[2][m] - F[3][m]) / T(24.0);
+  } else if (t == 1) {
+    for (int m = 0; m < 5; ++m) s[m] = (T(3.) * Q3[m] + T(6.) * Q4[m] - Q5[m]) / T(8.0);
+    flux_eq(1, s);
+    for (int m = 0; m < 5; ++m) {
+      s[m] = (T(-30.) * Q3[m] + T(145.) * Q4[m] + T(29.) * Q5[m] - T(8.) * Q6[m]) / T(136.0);
+      s2[m] = (T(2.) * Q3[m] + T(49.) * Q4[m] + T(125.) * Q5[m] - T(40.) * Q6[m]) / T(136.0);
+    }
+    flux_lr(2, s, s2);
+    for (int m = 0; m < 5; ++m) s[m] = (-Q4[m] + T(6.) * Q5[m] + T(3.) * Q6[m]) / T(8.0);
+    flux_eq(3, s);
+    for (int m = 0; m < 5; ++m) s[m] = (Q4[m] + T(2.) * Q5[m] + T(5.) * Q6[m]) / T(8.0);
+    flux_eq(4, s);
+    for (int m = 0; m < 5; ++m) s[m] = (Q4[m] + Q5[m] + T(6.) * Q6[m]) / T(8.0);
+    flux_eq(5, s);
+    for (int m = 0; m < 5; ++m)
+      fc[m] = (T(-22.) * F[1][m] + T(17.) * F[2][m] + T(9.) * F[3][m] - T(5.) * F[4][m] + F[5][m]) / T(24.0);
+  } else {
+    // face 1: left from round 2, right restored (fixed 5,15,-5,1 stencil)
+    for (int m = 0; m < 5; ++m) {
+      s[m] = (T(3.) * Q3[m] + T(6.) * Q4[m] - Q5[m]) / T(8.0);
+      s2[m] = (T(5.) * Q3[m] + T(15.) * Q4[m] - T(5.) * Q5[m] + Q6[m]) / T(16.);
+    }
+    flux_lr(1, s, s2);
+    // faces 2..4: right restored = WCNS right state of the main pass
+    for (int f = 2; f <= 4; ++f) {
+      for (int m = 0; m < 5; ++m) {
+        if (f == 2) s[m] = (T(-29.) * Q3[m] + T(170.) * Q4[m] + T(63.) * Q5[m] + T(12.) * Q6[m]) / T(216.0);
+        else if (f == 3) s[m] = (-Q4[m] + T(6.) * Q5[m] + T(3.) * Q6[m]) / T(8.0);
+        else s[m] = (Q4[m] + T(2.) * Q5[m] + T(5.) * Q6[m]) / T(8.0);
+        s2[m] = wcns_right<T>(ln.q(f + 1, m), ln.q(f + 2, m), ln.q(f + 3, m), ln.q(f + 4, m), ln.q(f + 5, m));
+      }
+      flux_lr(f, s, s2);
+    }
+    for (int m = 0; m < 5; ++m) fc[m] = (F[1][m] - T(27.) * F[2][m] + T(27.) * F[3][m] - F[4][m]) / T(24.0);
+  }
+}
+
+// Right-end re-calculation rounds (InviscidFluxComputer.cpp:450-521): fc[t] for
+// t = L-1, L-2, L-3.  Faces are stored at F[N - f'] with f' the face index.
+template <int D, typename S, typename T>
+__device__ void cascade_right(const BlockDev<S>& B, const InvLine<S, T>& ln, int t, T gamma, T fc[5]) {
+  const int N = ln.L;
+  T F[6][5];  // F[a] = flux at face N - a
+  auto flux_at = [&](int f, const T l[5], const T r[5]) {
+    T ql[5], qr[5];
+    for (int m = 0; m < 5; ++m) { ql[m] = l[m]; qr[m] = r[m]; }
+    T kx, ky, kz;
+    face_metric<D, S, T>(B, ln.o, ln.st, f, ln.L, kx, ky, kz);
+    fallback_roe<S, T>(ln, f, ql, qr, kx, ky, kz, gamma, F[N - f]);
+  };
+  T Qn[5], Qn1[5], Qn2[5], Qn3[5];
+  for (int m = 0; m < 5; ++m) {
+    Qn[m] = ln.q(N + 2, m); Qn1[m] = ln.q(N + 1, m); Qn2[m] = ln.q(N, m); Qn3[m] = ln.q(N - 1, m);
+  }
+  T s[5], s2[5];
+  if (t == N - 1) {
+    for (int m = 0; m < 5; ++m) s[m] = (T(3.) * Qn[m] - T(1.) * Qn1[m]) / T(2.0);
+    flux_at(N, s, s);
+    for (int m = 0; m < 5; ++m) s[m] = (T(19.) * Qn[m] + T(25.) * Qn1[m] - T(2.) * Qn2[m]) / T(42.0);
+    flux_at(N - 1, s, s);
+    for (int m = 0; m < 5; ++m) s[m] = (T(4.) * Qn[m] + T(3.) * Qn1[m] + T(9.) * Qn2[m] + T(2.) * Qn3[m]) / T(18.0);
+    flux_at(N - 2, s, s);
+    for (int m = 0; m < 5; ++m) s[m] = (T(-2.) * Qn[m] + T(3.) * Qn1[m] + T(3.) * Qn2[m] + T(2.) * Qn3[m]) / T(6.0);
+    flux_at(N - 3, s, s);
+    for (int m = 0; m < 5; ++m)
+      fc[m] = -(T(-23.) * F[0][m] + T(21.) * F[1][m] + T(3.) * F[2][m] - F[3][m]) / T(24.0);
+  } else if (t == N - 2) {
+    for (int m = 0; m < 5; ++m) s[m] = (T(3.) * Qn[m] + T(6.) * Qn1[m] - Qn2[m]) / T(8.0);
+    flux_at(N - 1, s, s);
+    for (int m = 0; m < 5; ++m) {
+      s2[m] = (T(-30.) * Qn[m] + T(145.) * Qn1[m] + T(29.) * Qn2[m] - T(8.) * Qn3[m]) / T(136.0);  // right
+      s[m] = (T(2.) * Qn[m] + T(49.) * Qn1[m] + T(125.) * Qn2[m] - T(40.) * Qn3[m]) / T(136.0);    // left
+    }
+    flux_at(N - 2, s, s2);
+    for (int m = 0; m < 5; ++m) s[m] = (-Qn1[m] + T(6.) * Qn2[m] + T(3.) * Qn3[m]) / T(8.0);
+    flux_at(N - 3, s, s);
+    for (int m = 0; m < 5; ++m) s[m] = (Qn1[m] + T(2.) * Qn2[m] + T(5.) * Qn3[m]) / T(8.0);
+    flux_at(N - 4, s, s);
+    for (int m = 0; m < 5; ++m) s[m] = (Qn1[m] + Qn2[m] + T(6.) * Qn3[m]) / T(8.0);
+    flux_at(N - 5, s, s);
+    for (int m = 0; m < 5; ++m)
+      fc[m] = -(T(-22.) * F[1][m] + T(17.) * F[2][m] + T(9.) * F[3][m] - T(5.) * F[4][m] + F[5][m]) / T(24.0);
+  } else {
+    // face N-1: right from round 2, left restored (fixed 5,15,-5,1 stencil)
+    for (int m = 0; m < 5; ++m) {
+      s2[m] = (T(3.) * Qn[m] + T(6.) * Qn1[m] - Qn2[m]) / T(8.0);
+      s[m] = (T(5.) * Qn[m] + T(15.) * Qn1[m] - T(5.) * Qn2[m] + Qn3[m]) / T(16.);
+    }
+    flux_at(N - 1, s, s2);
+    for (int f = N - 2; f >= N - 4; --f) {
+      for (int m = 0; m < 5; ++m) {
+        if (f == N - 2) s2[m] = (T(-29.) * Qn[m] + T(170.) * Qn1[m] + T(63.) * Qn2[m] + T(12.) * Qn3[m]) / T(216.0);
+        else if (f == N - 3) s2[m] = (-Qn1[m] + T(6.) * Qn2[m] + T(3.) * Qn3[m]) / T(8.0);
+        else s2[m] = (Qn1[m] + T(2.) * Qn2[m] + T(5.) * Qn3[m]) / T(8.0);
+        s[m] = wcns_left<T>(ln.q(f, m), ln.q(f + 1, m), ln.q(f + 2, m), ln.q(f + 3, m), ln.q(f + 4, m));
+      }
+      flux_at(f, s, s2);
+    }
+    for (int m = 0; m < 5; ++m) fc[m] = -(F[1][m] - T(27.) * F[2][m] + T(27.) * F[3][m] - F[4][m]) / T(24.0);
+  }
+}
+
+template <int D, typename S, typename T>
+__global__ void k_inviscid(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles, ParamsDev P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* fsh = reinterpret_cast<T*>(smem_raw);
+  const LineTile tl = tiles[blockIdx.x];
+  const BlockDev<S> B = blocks[tl.block];
+  const int L = dim_along(B, D);
+  const int nf = L + 1;
+  const long long st = stride_along(B, D);
+  const T gamma = T(P.gamma);
+  const int nitems = tl.count * nf;
+  for (int it = threadIdx.x; it < nitems; it += blockDim.x) {
+    int lane, f;
+    tile_item<D>(it, tl.count, nf, lane, f);
+    const long long o = line_origin(B, D, tl.first + lane);
+    InvLine<S, T> ln{B.prim, o, st, B.npad, L};
+    const bool fl = B.prim[o] < 1.0e-20;
+    const bool fr = B.prim[o + (long long)(L + 5) * st] < 1.0e-20;
+    T ql[5], qr[5], kx, ky, kz, fo[5];
+    initial_states<S, T>(ln, f, fl, fr, ql, qr);
+    face_metric<D, S, T>(B, o, st, f, L, kx, ky, kz);
+    fallback_roe<S, T>(ln, f, ql, qr, kx, ky, kz, gamma, fo);
+    T* dst = fsh + ((size_t)lane * nf + f) * 5;
+    for (int m = 0; m < 5; ++m) dst[m] = fo[m];
+  }
+  __syncthreads();
+  const int npts = tl.count * L;
+  for (int it = threadIdx.x; it < npts; it += blockDim.x) {
+    int lane, t;
+    tile_item<D>(it, tl.count, L, lane, t);
+    const long long o = line_origin(B, D, tl.first + lane);
+    const long long idx = o + (long long)(t + NG) * st;
+    const bool fl = B.prim[o] < 1.0e-20;
+    const bool fr = B.prim[o + (long long)(L + 5) * st] < 1.0e-20;
+    T fc[5];
+    if (fl && t <= 2) {
+      InvLine<S, T> ln{B.prim, o, st, B.npad, L};
+      cascade_left<D, S, T>(B, ln, t, gamma, fc);
+    } else if (fr && t >= L - 3) {
+      InvLine<S, T> ln{B.prim, o, st, B.npad, L};
+      cascade_right<D, S, T>(B, ln, t, gamma, fc);
+    } else {
+      const T* fb = fsh + (size_t)lane * nf * 5;
+      for (int m = 0; m < 5; ++m) fc[m] = flux_diff<T>(fb + m, 5, t, L);
+    }
+    for (int m = 0; m < 5; ++m) {
+      S* q = B.dq + m * B.npad + idx;
+      *q = (S)((T)*q + fc[m]);
+    }
+  }
+}
+
+// ===========================================================================
+// Interface residual averaging (HaloExchanger::average_interface_residuals,
+// src/solver/HaloExchanger.cpp:186-398): pack dq/vol of every source window
+// before any update, then each destination point applies its partners in
+// region order: dq = 0.5 * (dens_t * vol + dq).
+// ===========================================================================
+template <typename S>
+__global__ void k_iface_pack(const BlockDev<S>* __restrict__ blocks, const int* __restrict__ pk_block,
+                             const long long* __restrict__ pk_idx, double* __restrict__ pack, int n) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const BlockDev<S> B = blocks[pk_block[t]];
+  const long long idx = pk_idx[t];
+  const double vol = B.vol[idx];
+  for (int m = 0; m < 5; ++m) pack[(long long)t * 5 + m] = (double)B.dq[m * B.npad + idx] / vol;
+}
+
+template <typename S>
+__global__ void k_iface_apply(const BlockDev<S>* __restrict__ blocks, const int* __restrict__ ap_block,
+                              const long long* __restrict__ ap_idx, const int* __restrict__ ap_off,
+                              const int* __restrict__ ap_slot, const double* __restrict__ pack, int n) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const BlockDev<S> B = blocks[ap_block[t]];
+  const long long idx = ap_idx[t];
+  const double vol_s = B.vol[idx];
+  double q[5];
+  for (int m = 0; m < 5; ++m) q[m] = (double)B.dq[m * B.npad + idx];
+  for (int e = ap_off[t]; e < ap_off[t + 1]; ++e) {
+    const long long sl = ap_slot[e];
+    for (int m = 0; m < 5; ++m) {
+      const double dens_t = pack[sl * 5 + m];
+      q[m] = (double)(S)(0.5 * (dens_t * vol_s + q[m]));
+    }
+  }
+  for (int m = 0; m < 5; ++m) B.dq[m * B.npad + idx] = (S)q[m];
+}
+
+// ===========================================================================
+// LU-SGS / symmetric Gauss-Seidel (StateUpdater::update_solution,
+// src/solver/StateUpdater.cpp:267-580).
+// ===========================================================================
+// Prep: rhs = dq with physical-BC windows zeroed (set_boundary_dq_zero + the
+// AoS copy), and the diagonal coefficient 1/(1/dt + sum of radii)
+// (get_diag_coeff :267-295), which is the same in all four sweeps.
+template <typename S, typename T>
+__global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P) {
+  const Chunk ch = chunks[blockIdx.x];
+  const BlockDev<S> B = blocks[ch.block];
+  const long long np = B.npad;
+  const T gamma = T(P.gamma), reynolds = T(P.reynolds);
+  for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+    const long long n = ch.start + t;
+    const int ii = (int)(n % B.ni), jj = (int)((n / B.ni) % B.nj), kk = (int)(n / ((long long)B.ni * B.nj));
+    const long long idx = lin(B, NG + ii, NG + jj, NG + kk);
+    const bool masked = B.bcmask[idx] != 0;
+    for (int m = 0; m < 5; ++m) B.rhs[m * np + idx] = masked ? (S)0 : B.dq[m * np + idx];
+    const T rho = (T)B.prim[idx], u = (T)B.prim[np + idx], v = (T)B.prim[2 * np + idx], w = (T)B.prim[3 * np + idx],
+            p = (T)B.prim[4 * np + idx];
+    T km[9];
+    for (int m = 0; m < 9; ++m) km[m] = (T)B.metrics[m * np + idx];
+    const T ra = spectral_radius<T>(rho, u, v, w, p, gamma, km[0], km[1], km[2]);
+    const T rb = spectral_radius<T>(rho, u, v, w, p, gamma, km[3], km[4], km[5]);
+    const T rc = spectral_radius<T>(rho, u, v, w, p, gamma, km[6], km[7], km[8]);
+    T rva = T(0), rvb = T(0), rvc = T(0);
+    if (P.nvis == 1) {
+      const T mu = (T)B.mu[idx];
+      T vol = (T)B.vol[idx];
+      if (vol < T(1e-30)) vol = T(1e-30);
+      rva = visc_spectral_radius<T>(rho, mu, vol, reynolds, km[0], km[1], km[2]);
+      rvb = visc_spectral_radius<T>(rho, mu, vol, reynolds, km[3], km[4], km[5]);
+      rvc = visc_spectral_radius<T>(rho, mu, vol, reynolds, km[6], km[7], km[8]);
+    }
+    const T rad_sum = ra + rb + rc + rva + rvb + rvc;
+    const T term = (T(1) / (T)B.dt[idx]) + rad_sum;
+    B.coed[idx] = (S)(T(1) / term);
+  }
+}
+
+enum SweepMode { SW_LUSGS_FWD = 0, SW_LUSGS_BWD = 1, SW_GS = 2 };
+
+// Neighbour contribution (add_nb / add_nb_contrib, StateUpdater.cpp:326-347, 401-426).
+template <typename S, typename T, int MODE>
+__device__ __forceinline__ void sweep_nb(const BlockDev<S>& B, const ParamsDev& P, long long nidx, const T km[3],
+                                         T sgn, T rhs0[5]) {
+  const long long np = B.npad;
+  T pn[5], dn[5];
+  for (int m = 0; m < 5; ++m) {
+    pn[m] = (T)B.prim[m * np + nidx];
+    dn[m] = (T)B.dq[m * np + nidx];
+  }
+  const T gamma = T(P.gamma);
+  const T r = spectral_radius<T>(pn[0], pn[1], pn[2], pn[3], pn[4], gamma, km[0], km[1], km[2]);
+  T fs[5];
+  flux_split<T>(pn, dn, km[0], km[1], km[2], r, sgn, gamma, fs);
+  if (P.nvis == 1) {
+    const T mu_nb = (T)B.mu[nidx];
+    T vol_nb = (T)B.vol[nidx];
+    if (vol_nb < T(1e-30)) vol_nb = T(1e-30);
+    const T rv = visc_spectral_radius<T>(pn[0], mu_nb, vol_nb, T(P.reynolds), km[0], km[1], km[2]);
+    if (MODE == SW_GS) {
+      for (int m = 0; m < 5; ++m) fs[m] += T(0.5) * rv * dn[m] * sgn;
+    } else {
+      for (int m = 0; m < 5; ++m) fs[m] += T(0.5) * rv * dn[m];
+    }
+  }
+  if (MODE == SW_GS && sgn < T(0)) {
+    for (int m = 0; m < 5; ++m) rhs0[m] -= fs[m];
+  } else {
+    for (int m = 0; m < 5; ++m) rhs0[m] += fs[m];
+  }
+}
+
+template <typename S, typename T, int MODE>
+__device__ __forceinline__ void sweep_point(const BlockDev<S>& B, const ParamsDev& P, int ii, int jj, int kk) {
+  const long long np = B.npad;
+  const long long idx = lin(B, NG + ii, NG + jj, NG + kk);
+  const long long sj = B.nx, sk = (long long)B.nx * B.ny;
+  T km[9];
+  for (int m = 0; m < 9; ++m) km[m] = (T)B.metrics[m * np + idx];
+  T rhs0[5] = {T(0), T(0), T(0), T(0), T(0)};
+  if (MODE == SW_LUSGS_FWD || MODE == SW_GS) {
+    if (ii > 0) sweep_nb<S, T, MODE>(B, P, idx - 1, km + 0, T(1), rhs0);
+    if (jj > 0) sweep_nb<S, T, MODE>(B, P, idx - sj, km + 3, T(1), rhs0);
+    if (kk > 0) sweep_nb<S, T, MODE>(B, P, idx - sk, km + 6, T(1), rhs0);
+  }
+  if (MODE == SW_LUSGS_BWD || MODE == SW_GS) {
+    if (ii < B.ni - 1) sweep_nb<S, T, MODE>(B, P, idx + 1, km + 0, T(-1), rhs0);
+    if (jj < B.nj - 1) sweep_nb<S, T, MODE>(B, P, idx + sj, km + 3, T(-1), rhs0);
+    if (kk < B.nk - 1) sweep_nb<S, T, MODE>(B, P, idx + sk, km + 6, T(-1), rhs0);
+  }
+  const T coed = (T)B.coed[idx];
+  for (int m = 0; m < 5; ++m) {
+    S* d = B.dq + m * np + idx;
+    if (MODE == SW_LUSGS_FWD) {
+      const T explicit_term = -(T)B.rhs[m * np + idx];
+      *d = (S)((explicit_term + rhs0[m]) * coed);
+    } else if (MODE == SW_LUSGS_BWD) {
+      *d = (S)((T)*d - rhs0[m] * coed);
+    } else {
+      const T resid = -(T)B.rhs[m * np + idx];
+      *d = (S)((rhs0[m] + resid) * coed);
+    }
+  }
+}
+
+// One i+j+k hyperplane of one sweep for every block: points with ii+jj+kk == s.
+template <typename S, typename T, int MODE>
+__global__ void k_sweep_plane(const BlockDev<S>* __restrict__ blocks, const PlaneChunk* __restrict__ chunks, ParamsDev P,
+                              int s_fwd, int backward) {
+  const PlaneChunk ch = chunks[blockIdx.x];
+  const BlockDev<S> B = blocks[ch.block];
+  const int t = threadIdx.x;
+  if (t >= ch.count) return;
+  const int smax = B.ni + B.nj + B.nk - 3;
+  const int s = backward ? (smax - s_fwd) : s_fwd;
+  if (s < 0 || s > smax) return;
+  const int n = ch.start + t;
+  const int jj = n % B.nj, kk = n / B.nj;
+  const int ii = s - jj - kk;
+  if (ii < 0 || ii >= B.ni) return;
+  sweep_point<S, T, MODE>(B, P, ii, jj, kk);
+}
+
+// ===========================================================================
+// Final update: set_boundary_dq_zero + update_limited (StateUpdater.cpp:447-542),
+// optionally fused with the residual (ResidualMonitor::compute,
+// src/solver/ResidualMonitor.cpp:11-137): per-CTA partial sums and maxima with
+// the lexicographic location key; a single CTA combines them in fixed order.
+// ===========================================================================
+template <typename S>
+__device__ __forceinline__ void limited_update(const BlockDev<S>& B, const ParamsDev& P, long long idx,
+                                               const double dq[5]) {
+  const long long np = B.npad;
+  const double gm1 = P.gamma - 1.0;
+  const double r = B.prim[idx], u = B.prim[np + idx], v = B.prim[2 * np + idx], w = B.prim[3 * np + idx],
+               p = B.prim[4 * np + idx];
+  const double E = p / gm1 + 0.5 * r * (u * u + v * v + w * w);
+  double qn[5];
+  qn[0] = r + dq[0];
+  qn[1] = r * u + dq[1];
+  qn[2] = r * v + dq[2];
+  qn[3] = r * w + dq[3];
+  qn[4] = E + dq[4];
+  double r_n = qn[0];
+  double inv_r = 1.0 / r_n;
+  const double a = qn[1] * inv_r, b = qn[2] * inv_r, c = qn[3] * inv_r;
+  const double p_n = gm1 * (qn[4] - 0.5 * r_n * (a * a + b * b + c * c));
+  const double dp_p = fabs((p_n - p) / p);
+  const double term = tmax(0.0, -0.3 + dp_p);
+  const double Fa = 1.0 / (1.0 + 2.0 * term);
+  double qf[5];
+  qf[0] = r + dq[0] * Fa;
+  qf[1] = r * u + dq[1] * Fa;
+  qf[2] = r * v + dq[2] * Fa;
+  qf[3] = r * w + dq[3] * Fa;
+  qf[4] = E + dq[4] * Fa;
+  r_n = qf[0];
+  inv_r = 1.0 / r_n;
+  const double u_n = qf[1] * inv_r, v_n = qf[2] * inv_r, w_n = qf[3] * inv_r;
+  const double p_nf = gm1 * (qf[4] - 0.5 * r_n * (u_n * u_n + v_n * v_n + w_n * w_n));
+  if (!(r_n <= 1e-6 || p_nf <= 1e-6)) {
+    B.prim[idx] = r_n;
+    B.prim[np + idx] = u_n;
+    B.prim[2 * np + idx] = v_n;
+    B.prim[3 * np + idx] = w_n;
+    B.prim[4 * np + idx] = p_nf;
+  }
+}
+
+__device__ __forceinline__ void res_combine(double& sum, double& mx, long long& key, double osum, double omx,
+                                            long long okey) {
+  sum += osum;
+  if (omx > mx || (omx == mx && okey < key)) {
+    mx = omx;
+    key = okey;
+  }
+}
+
+template <int NT>
+__device__ __forceinline__ void block_reduce_res(double& sum, double& mx, long long& key) {
+  // warp then CTA tree, fixed shape => deterministic
+  for (int off = 16; off > 0; off >>= 1) {
+    const double os = __shfl_down_sync(0xffffffffu, sum, off);
+    const double om = __shfl_down_sync(0xffffffffu, mx, off);
+    const long long ok = __shfl_down_sync(0xffffffffu, key, off);
+    res_combine(sum, mx, key, os, om, ok);
+  }
+  __shared__ double s_sum[NT / 32];
+  __shared__ double s_max[NT / 32];
+  __shared__ long long s_key[NT / 32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    s_sum[w] = sum;
+    s_max[w] = mx;
+    s_key[w] = key;
+  }
+  __syncthreads();
+  if (w == 0) {
+    sum = (l < NT / 32) ? s_sum[l] : 0.0;
+    mx = (l < NT / 32) ? s_max[l] : -1.0;
+    key = (l < NT / 32) ? s_key[l] : (long long)0x7fffffffffffffffLL;
+    for (int off = 16; off > 0; off >>= 1) {
+      const double os = __shfl_down_sync(0xffffffffu, sum, off);
+      const double om = __shfl_down_sync(0xffffffffu, mx, off);
+      const long long ok = __shfl_down_sync(0xffffffffu, key, off);
+      res_combine(sum, mx, key, os, om, ok);
+    }
+  }
+}
+
+template <typename S, bool DO_UPDATE, bool DO_RES, int NT>
+__global__ void __launch_bounds__(NT) k_update_res(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks,
+                                                   ParamsDev P, ResPartial* __restrict__ partials) {
+  const Chunk ch = chunks[blockIdx.x];
+  const BlockDev<S> B = blocks[ch.block];
+  const long long np = B.npad;
+  double sum = 0.0, mx = -1.0;
+  long long key = (long long)0x7fffffffffffffffLL;
+  for (int t = threadIdx.x; t < ch.count; t += NT) {
+    const long long n = ch.start + t;
+    const int ii = (int)(n % B.ni), jj = (int)((n / B.ni) % B.nj), kk = (int)(n / ((long long)B.ni * B.nj));
+    const long long idx = lin(B, NG + ii, NG + jj, NG + kk);
+    double dq[5];
+    if (DO_UPDATE && B.bcmask[idx]) {
+      for (int m = 0; m < 5; ++m) {
+        B.dq[m * np + idx] = (S)0;
+        dq[m] = 0.0;
+      }
+    } else {
+      for (int m = 0; m < 5; ++m) dq[m] = (double)B.dq[m * np + idx];
+    }
+    if (DO_UPDATE) limited_update(B, P, idx, dq);
+    if (DO_RES) {
+      double vol = B.vol[idx];
+      double dt = (double)B.dt[idx];
+      if (vol < 1e-30) vol = 1e-30;
+      if (dt < 1e-30) dt = 1e-30;
+      const double inv_factor = 1.0 / (dt * vol);
+      const long long kbase = (B.int_base + n) * 5;
+      for (int m = 0; m < 5; ++m) {
+        const double res = fabs(dq[m]) * inv_factor;
+        sum += res * res;
+        if (res > mx) {
+          mx = res;
+          key = kbase + m;
+        }
+      }
+    }
+  }
+  if (DO_RES) {
+    block_reduce_res<NT>(sum, mx, key);
+    if (threadIdx.x == 0) partials[blockIdx.x] = ResPartial{sum, mx, key};
+  }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(1024) k_res_final(const BlockDev<S>* __restrict__ blocks, int nblocks,
+                                                     const ResPartial* __restrict__ partials, int npart,
+                                                     long long total_points, const unsigned long long* dtmin_bits,
+                                                     ResidualOut* __restrict__ hist, int* __restrict__ counter,
+                                                     int capacity) {
+  double sum = 0.0, mx = -1.0;
+  long long key = (long long)0x7fffffffffffffffLL;
+  for (int t = threadIdx.x; t < npart; t += 1024) {
+    const ResPartial p = partials[t];
+    res_combine(sum, mx, key, p.sum, p.max, p.key);
+  }
+  block_reduce_res<1024>(sum, mx, key);
+  if (threadIdx.x == 0) {
+    ResidualOut r;
+    r.rms = total_points > 0 ? sqrt(sum / (double)total_points) : 0.0;
+    r.max = mx;
+    const long long pt = key / 5;
+    int b = 0;
+    for (int q = 0; q < nblocks; ++q) {
+      const BlockDev<S>& B = blocks[q];
+      if (pt >= B.int_base && pt < B.int_base + (long long)B.ni * B.nj * B.nk) b = q;
+    }
+    const BlockDev<S>& B = blocks[b];
+    const long long n = pt - B.int_base;
+    r.loc[0] = b;
+    r.loc[1] = (int)(n % B.ni) + 1;
+    r.loc[2] = (int)((n / B.ni) % B.nj) + 1;
+    r.loc[3] = (int)(n / ((long long)B.ni * B.nj)) + 1;
+    r.loc[4] = (int)(key % 5) + 1;
+    r.pad = 0;
+    r.phydtime = __longlong_as_double((long long)*dtmin_bits);
+    const int c = *counter;
+    hist[c % capacity] = r;
+    *counter = c + 1;
+  }
+}
+
+// ===========================================================================
+// Initial flow on the device: freestream + splitmix64 noise + EOS temperature
+// (initialize_flow / update_temperature, src/preprocess/InitialCondition.cpp:7-147).
+// ===========================================================================
+__device__ __forceinline__ double splitmix_uniform(unsigned long long seed, unsigned long long n) {
+  unsigned long long z = seed + n * 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z = z ^ (z >> 31);
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+template <typename S>
+__global__ void k_init_flow(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks,
+                            const long long* __restrict__ pad_base, ParamsDev P, unsigned long long seed, double amp) {
+  const Chunk ch = chunks[blockIdx.x];
+  const BlockDev<S> B = blocks[ch.block];
+  const long long np = B.npad;
+  for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+    const long long idx = ch.start + t;
+    const unsigned long long n = (unsigned long long)(pad_base[ch.block] + idx);
+    double rho = P.roo, u = P.uoo;
+    if (amp != 0.0) {
+      const double r1 = splitmix_uniform(seed, 2 * n + 1);
+      const double r2 = splitmix_uniform(seed, 2 * n + 2);
+      rho = rho * (1.0 + amp * (2.0 * r1 - 1.0));
+      u = u * (1.0 + amp * (2.0 * r2 - 1.0));
+    }
+    const double p = P.poo;
+    B.prim[idx] = rho;
+    B.prim[np + idx] = u;
+    B.prim[2 * np + idx] = P.voo;
+    B.prim[3 * np + idx] = P.woo;
+    B.prim[4 * np + idx] = p;
+    double T = P.too;
+    if (P.nvis == 1) {
+      double r = rho;
+      if (r < 1.0e-30) r = 1.0e-30;
+      const double a2 = P.gamma * p / r;
+      T = (P.moo * P.moo) * a2;
+    }
+    B.prim[5 * np + idx] = T;
+    B.q[idx] = P.roo;
+    B.q[np + idx] = P.roo * P.uoo;
+    B.q[2 * np + idx] = P.roo * P.voo;
+    B.q[3 * np + idx] = P.roo * P.woo;
+    const double v2 = P.uoo * P.uoo + P.voo * P.voo + P.woo * P.woo;
+    B.q[4 * np + idx] = P.poo / (P.gamma - 1.0) + 0.5 * P.roo * v2;
+    for (int m = 0; m < 5; ++m) B.dq[m * np + idx] = (S)0;
+  }
+}
+
+}  // namespace orion

@@ -1,0 +1,1011 @@
+// C-ABI runtime of the B200 per-step path: case lifetime, work lists, stage
+// launchers and the graph-captured step.  See include/orion_gpu.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "orion_gpu.h"
+#include "topology.hpp"
+
+using namespace orion;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                       \
+  do {                                                                                       \
+    cudaError_t _e = (expr);                                                                 \
+    if (_e != cudaSuccess)                                                                   \
+      return fail(ORION_E_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e));         \
+  } while (0)
+
+constexpr int kThreads = 256;
+constexpr int kChunk = 1024;        // points per CTA for pointwise kernels
+constexpr int kHistCap = 4096;      // residual history ring
+constexpr size_t kLineSmemBudget = 96 * 1024;
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+struct DeviceLists {
+  Chunk* pad_chunks = nullptr;
+  int n_pad_chunks = 0;
+  Chunk* int_chunks = nullptr;
+  int n_int_chunks = 0;
+  LineTile* tiles[3] = {nullptr, nullptr, nullptr};
+  int n_tiles[3] = {0, 0, 0};
+  int lanes[3] = {1, 1, 1};
+  int lmax[3] = {0, 0, 0};
+  PlaneChunk* plane_chunks = nullptr;
+  int n_plane_chunks = 0;
+  int max_planes = 0;
+  long long* halo_src = nullptr;
+  long long* halo_dst = nullptr;
+  int n_halo = 0;
+  RegionDev* regions = nullptr;
+  int* phase_regions = nullptr;
+  std::vector<int> phase_off;  // host: region list offsets per phase
+  std::vector<int> phase_maxpts;
+  int* pk_block = nullptr;
+  long long* pk_idx = nullptr;
+  double* pack = nullptr;
+  int n_pack = 0;
+  int* ap_block = nullptr;
+  long long* ap_idx = nullptr;
+  int* ap_off = nullptr;
+  int* ap_slot = nullptr;
+  int n_ap = 0;
+  ResPartial* partials = nullptr;
+  ResidualOut* hist = nullptr;
+  int* counter = nullptr;
+  unsigned long long* dtmin = nullptr;
+  long long* pad_base = nullptr;
+};
+
+}  // namespace
+
+struct orion_case_s {
+  int nblocks = 0;
+  int prec = ORION_PREC_FP64;
+  ParamsDev P{};
+  std::vector<HostBlock> hb;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int device = 0;
+  void* arena = nullptr;
+  size_t arena_bytes = 0;
+  std::vector<void*> allocs;  // other device allocations
+  std::vector<BlockDev<double>> bd64;
+  std::vector<BlockDev<float>> bd32;
+  void* d_blocks = nullptr;
+  DeviceLists L;
+  long long total_interior = 0;
+  cudaGraphExec_t graph = nullptr;
+  long long steps_done = 0;
+};
+
+namespace {
+
+template <typename T>
+int dev_upload(orion_case_t c, T** dptr, const std::vector<T>& v) {
+  *dptr = nullptr;
+  if (v.empty()) return 0;
+  void* p = nullptr;
+  if (cudaMalloc(&p, v.size() * sizeof(T)) != cudaSuccess) return fail(ORION_E_NOMEM, "cudaMalloc (work list)");
+  c->allocs.push_back(p);
+  CUDA_TRY(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *dptr = static_cast<T*>(p);
+  return 0;
+}
+
+template <typename T>
+int dev_alloc(orion_case_t c, T** dptr, size_t n) {
+  void* p = nullptr;
+  if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return fail(ORION_E_NOMEM, "cudaMalloc");
+  c->allocs.push_back(p);
+  CUDA_TRY(cudaMemset(p, 0, std::max<size_t>(n, 1) * sizeof(T)));
+  *dptr = static_cast<T*>(p);
+  return 0;
+}
+
+// Bytes of one block's fields for storage size ssz.
+size_t block_bytes(const HostBlock& b, size_t ssz) {
+  const size_t np = (size_t)b.npad;
+  size_t s = 0;
+  auto add = [&](size_t bytes) { s = align_up(s, 256) + bytes; };
+  add(6 * np * 8);    // prim
+  add(5 * np * 8);    // q
+  add(5 * np * ssz);  // dq
+  add(9 * np * 8);    // metrics
+  add(np * 8);        // vol
+  add(np * ssz);      // dt
+  add(np * ssz);      // c
+  add(np * ssz);      // mu
+  add(5 * np * ssz);  // rhs
+  add(np * ssz);      // coed
+  add(12 * np * ssz); // duvwt
+  add(np);            // bcmask
+  return align_up(s, 256);
+}
+
+template <typename S>
+void carve_block(char* base, const HostBlock& b, BlockDev<S>& d) {
+  const size_t np = (size_t)b.npad;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    off = align_up(off, 256);
+    char* p = base + off;
+    off += bytes;
+    return p;
+  };
+  d.prim = reinterpret_cast<double*>(take(6 * np * 8));
+  d.q = reinterpret_cast<double*>(take(5 * np * 8));
+  d.dq = reinterpret_cast<S*>(take(5 * np * sizeof(S)));
+  d.metrics = reinterpret_cast<double*>(take(9 * np * 8));
+  d.vol = reinterpret_cast<double*>(take(np * 8));
+  d.dt = reinterpret_cast<S*>(take(np * sizeof(S)));
+  d.c = reinterpret_cast<S*>(take(np * sizeof(S)));
+  d.mu = reinterpret_cast<S*>(take(np * sizeof(S)));
+  d.rhs = reinterpret_cast<S*>(take(5 * np * sizeof(S)));
+  d.coed = reinterpret_cast<S*>(take(np * sizeof(S)));
+  d.duvwt = reinterpret_cast<S*>(take(12 * np * sizeof(S)));
+  d.bcmask = reinterpret_cast<uint8_t*>(take(np));
+  d.ni = b.idim;
+  d.nj = b.jdim;
+  d.nk = b.kdim;
+  d.nx = b.nx;
+  d.ny = b.ny;
+  d.nz = b.nz;
+  d.npad = b.npad;
+}
+
+int validate_blocks(int nblocks, const orion_block_desc_t* blocks) {
+  if (nblocks <= 0 || !blocks) return fail(ORION_E_INVALID, "nblocks must be positive");
+  for (int b = 0; b < nblocks; ++b) {
+    const auto& d = blocks[b];
+    if (d.idim < 12 || d.jdim < 12 || d.kdim < 12)
+      return fail(ORION_E_UNSUPPORTED, "block " + std::to_string(b) + ": every extent must be >= 12 points");
+    if (d.nregions < 0 || (d.nregions > 0 && !d.regions))
+      return fail(ORION_E_INVALID, "block " + std::to_string(b) + ": bad region list");
+    for (int r = 0; r < d.nregions; ++r) {
+      const auto& g = d.regions[r];
+      if (g.bctype < 0 && (g.nbt < 1 || g.nbt > nblocks || g.ibcwin < 1))
+        return fail(ORION_E_INVALID, "block " + std::to_string(b) + " region " + std::to_string(r) +
+                                         ": interface target out of range");
+    }
+  }
+  return 0;
+}
+
+// --------------------------------------------------------------------------
+// work-list builders
+// --------------------------------------------------------------------------
+int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
+  auto& L = c->L;
+  const int nb = c->nblocks;
+  // pointwise chunks over padded and interior index spaces
+  std::vector<Chunk> pad, itr;
+  std::vector<long long> pad_base(nb);
+  long long pb = 0;
+  for (int b = 0; b < nb; ++b) {
+    const auto& h = c->hb[b];
+    pad_base[b] = pb;
+    pb += h.npad;
+    for (long long s = 0; s < h.npad; s += kChunk) pad.push_back(Chunk{b, (int)std::min<long long>(kChunk, h.npad - s), s});
+    const long long ni = (long long)h.idim * h.jdim * h.kdim;
+    for (long long s = 0; s < ni; s += kChunk) itr.push_back(Chunk{b, (int)std::min<long long>(kChunk, ni - s), s});
+  }
+  int rc;
+  if ((rc = dev_upload(c, &L.pad_chunks, pad))) return rc;
+  L.n_pad_chunks = (int)pad.size();
+  if ((rc = dev_upload(c, &L.int_chunks, itr))) return rc;
+  L.n_int_chunks = (int)itr.size();
+  if ((rc = dev_upload(c, &L.pad_base, pad_base))) return rc;
+
+  // line tiles per direction
+  const size_t tsz = (c->prec == ORION_PREC_FP64) ? 8 : 4;
+  for (int d = 0; d < 3; ++d) {
+    int lmax = 0;
+    for (auto& h : c->hb) lmax = std::max(lmax, d == 0 ? h.idim : (d == 1 ? h.jdim : h.kdim));
+    L.lmax[d] = lmax;
+    int lanes = (int)std::min<size_t>(32, kLineSmemBudget / ((size_t)(lmax + 1) * 5 * tsz));
+    if (lanes < 1) return fail(ORION_E_UNSUPPORTED, "grid line too long for the line kernels");
+    if (d > 0 && lanes >= 8) lanes = lanes / 8 * 8;
+    L.lanes[d] = lanes;
+    std::vector<LineTile> tiles;
+    for (int b = 0; b < nb; ++b) {
+      const auto& h = c->hb[b];
+      const int nlines = d == 0 ? h.jdim * h.kdim : (d == 1 ? h.idim * h.kdim : h.idim * h.jdim);
+      for (int s = 0; s < nlines; s += lanes) tiles.push_back(LineTile{b, s, std::min(lanes, nlines - s), 0});
+    }
+    if ((rc = dev_upload(c, &L.tiles[d], tiles))) return rc;
+    L.n_tiles[d] = (int)tiles.size();
+  }
+
+  // wavefront plane chunks: (jj,kk) index space of every block
+  std::vector<PlaneChunk> pcs;
+  L.max_planes = 0;
+  for (int b = 0; b < nb; ++b) {
+    const auto& h = c->hb[b];
+    L.max_planes = std::max(L.max_planes, h.idim + h.jdim + h.kdim - 2);
+    const int n = h.jdim * h.kdim;
+    for (int s = 0; s < n; s += kThreads) pcs.push_back(PlaneChunk{b, s, std::min(kThreads, n - s), 0});
+  }
+  if ((rc = dev_upload(c, &L.plane_chunks, pcs))) return rc;
+  L.n_plane_chunks = (int)pcs.size();
+
+  // ---------------- halo copy (exchange_bc) ----------------
+  {
+    struct Msg {
+      int tb, tw;
+      std::vector<long long> src;
+    };
+    std::vector<Msg> queue;
+    for (int b = 0; b < nb; ++b) {
+      const auto& h = c->hb[b];
+      const int dims[3] = {h.idim, h.jdim, h.kdim};
+      for (const auto& hr : h.regions) {
+        if (hr.r.nbt <= 0) continue;
+        int beg[3], end[3];
+        memory_window(hr, NG, dims, 0, beg, end);
+        Msg msg{hr.r.nbt - 1, hr.r.ibcwin - 1, {}};
+        for (int m = 0; m < 5; ++m)
+          for (int k = beg[2]; k <= end[2]; ++k)
+            for (int j = beg[1]; j <= end[1]; ++j)
+              for (int i = beg[0]; i <= end[0]; ++i)
+                msg.src.push_back(prim_off[b] + m * h.npad + (i + (long long)h.nx * (j + (long long)h.ny * k)));
+        queue.push_back(std::move(msg));
+      }
+    }
+    std::map<long long, long long> dst2src;  // last writer wins
+    std::vector<long long> order;
+    for (int b = 0; b < nb; ++b) {
+      const auto& h = c->hb[b];
+      const int dims[3] = {h.idim, h.jdim, h.kdim};
+      for (int r = 0; r < (int)h.regions.size(); ++r) {
+        const auto& hr = h.regions[r];
+        if (hr.r.nbt <= 0) continue;
+        auto it = std::find_if(queue.begin(), queue.end(), [&](const Msg& q) { return q.tb == b && q.tw == r; });
+        if (it == queue.end())
+          return fail(ORION_E_INVALID, "interface block " + std::to_string(b) + " region " + std::to_string(r) +
+                                           " has no sending partner");
+        int beg[3], end[3];
+        memory_window(hr, NG, dims, 1, beg, end);
+        std::vector<long long> pts;
+        for (int k = beg[2]; k <= end[2]; ++k)
+          for (int j = beg[1]; j <= end[1]; ++j)
+            for (int i = beg[0]; i <= end[0]; ++i) pts.push_back(i + (long long)h.nx * (j + (long long)h.ny * k));
+        const size_t np = pts.size();
+        for (size_t q = 0; q < 5 * np && q < it->src.size(); ++q) {
+          const long long dst = prim_off[b] + (long long)(q / np) * h.npad + pts[q % np];
+          if (!dst2src.count(dst)) order.push_back(dst);
+          dst2src[dst] = it->src[q];
+        }
+        queue.erase(it);
+      }
+    }
+    std::vector<long long> hs, hd;
+    for (long long d : order) {
+      hd.push_back(d);
+      hs.push_back(dst2src[d]);
+    }
+    if ((rc = dev_upload(c, &L.halo_src, hs))) return rc;
+    if ((rc = dev_upload(c, &L.halo_dst, hd))) return rc;
+    L.n_halo = (int)hd.size();
+  }
+
+  // ---------------- physical BC phases ----------------
+  {
+    std::vector<std::vector<RegionDev>> per_block(nb);
+    for (int b = 0; b < nb; ++b) {
+      const auto& h = c->hb[b];
+      for (const auto& hr : h.regions) {
+        if (hr.r.bctype < 0) continue;
+        RegionDev R{};
+        R.block = b;
+        R.type = hr.r.bctype;
+        R.s_nd = hr.s_nd;
+        R.dir = hr.s_nd - 1;
+        R.lr = hr.s_lr;
+        if (R.dir < 0) return fail(ORION_E_UNSUPPORTED, "physical BC region is not a face");
+        for (int m = 0; m < 3; ++m) {
+          R.lo[m] = hr.r.s_st[m] - 1 + NG;
+          R.hi[m] = hr.r.s_ed[m] - 1 + NG;
+        }
+        const long long npts = (long long)std::max(0, R.hi[0] - R.lo[0] + 1) * std::max(0, R.hi[1] - R.lo[1] + 1) *
+                               std::max(0, R.hi[2] - R.lo[2] + 1);
+        R.npts = (int)npts;
+        R.is2d = (R.type == 3 && R.dir != 2 && h.kdim <= 2) ? 1 : 0;
+        per_block[b].push_back(R);
+      }
+    }
+    std::vector<RegionDev> regs;
+    std::vector<int> phase_list;
+    size_t nphase = 0;
+    for (auto& v : per_block) nphase = std::max(nphase, v.size());
+    L.phase_off.assign(1, 0);
+    L.phase_maxpts.clear();
+    for (size_t p = 0; p < nphase; ++p) {
+      int maxpts = 0;
+      for (int b = 0; b < nb; ++b) {
+        if (p < per_block[b].size()) {
+          phase_list.push_back((int)regs.size());
+          regs.push_back(per_block[b][p]);
+          maxpts = std::max(maxpts, per_block[b][p].npts);
+        }
+      }
+      L.phase_off.push_back((int)phase_list.size());
+      L.phase_maxpts.push_back(maxpts);
+    }
+    if ((rc = dev_upload(c, &L.regions, regs))) return rc;
+    if ((rc = dev_upload(c, &L.phase_regions, phase_list))) return rc;
+  }
+
+  // ---------------- interface residual averaging ----------------
+  {
+    struct Src {
+      int slot_base, n;
+    };
+    std::map<std::pair<int, int>, Src> qsrc;  // target (block, region) -> packing region
+    std::vector<int> pkb;
+    std::vector<long long> pki;
+    for (int b = 0; b < nb; ++b) {
+      const auto& h = c->hb[b];
+      for (int r = 0; r < (int)h.regions.size(); ++r) {
+        const auto& g = h.regions[r].r;
+        if (g.bctype >= 0) continue;
+        int lo[3], hi[3];
+        for (int d = 0; d < 3; ++d) {
+          lo[d] = std::min(std::abs(g.s_st[d]), std::abs(g.s_ed[d]));
+          hi[d] = std::max(std::abs(g.s_st[d]), std::abs(g.s_ed[d]));
+        }
+        Src s{(int)pkb.size(), 0};
+        for (int k = lo[2]; k <= hi[2]; ++k)
+          for (int j = lo[1]; j <= hi[1]; ++j)
+            for (int i = lo[0]; i <= hi[0]; ++i) {
+              pkb.push_back(b);
+              pki.push_back((i - 1 + NG) + (long long)h.nx * ((j - 1 + NG) + (long long)h.ny * (k - 1 + NG)));
+              s.n++;
+            }
+        qsrc[{g.nbt - 1, g.ibcwin - 1}] = s;
+      }
+    }
+    std::map<std::pair<int, long long>, std::vector<int>> entries;
+    std::vector<std::pair<int, long long>> dorder;
+    for (int b = 0; b < nb; ++b) {
+      const auto& h = c->hb[b];
+      for (int r = 0; r < (int)h.regions.size(); ++r) {
+        const auto& hr = h.regions[r];
+        const auto& g = hr.r;
+        if (g.bctype >= 0) continue;
+        auto it = qsrc.find({b, r});
+        if (it == qsrc.end())
+          return fail(ORION_E_INVALID, "interface block " + std::to_string(b) + " region " + std::to_string(r) +
+                                           " receives no averaging data");
+        std::vector<std::array<int, 3>> img;
+        int md[3];
+        interface_image(hr, img, md);
+        int slo[3], tlo[3], thi[3];
+        for (int d = 0; d < 3; ++d) {
+          slo[d] = std::min(std::abs(g.s_st[d]), std::abs(g.s_ed[d]));
+          tlo[d] = std::min(std::abs(g.t_st[d]), std::abs(g.t_ed[d]));
+          thi[d] = std::max(std::abs(g.t_st[d]), std::abs(g.t_ed[d]));
+        }
+        const int nxt = thi[0] - tlo[0] + 1, nyt = thi[1] - tlo[1] + 1;
+        for (int k = 0; k < md[2]; ++k)
+          for (int j = 0; j < md[1]; ++j)
+            for (int i = 0; i < md[0]; ++i) {
+              const auto& t = img[(size_t)i + (size_t)md[0] * ((size_t)j + (size_t)md[1] * k)];
+              const long long rem =
+                  (long long)(t[0] - tlo[0]) + (long long)nxt * ((t[1] - tlo[1]) + (long long)nyt * (t[2] - tlo[2]));
+              if (rem < 0 || rem >= it->second.n)
+                return fail(ORION_E_UNSUPPORTED, "interface averaging map leaves the partner window");
+              const long long idx = (slo[0] + i - 1 + NG) +
+                                    (long long)h.nx * ((slo[1] + j - 1 + NG) + (long long)h.ny * (slo[2] + k - 1 + NG));
+              auto key = std::make_pair(b, idx);
+              auto& e = entries[key];
+              if (e.empty()) dorder.push_back(key);
+              e.push_back(it->second.slot_base + (int)rem);
+            }
+      }
+    }
+    std::vector<int> apb, apo{0}, aps;
+    std::vector<long long> api;
+    for (auto& key : dorder) {
+      apb.push_back(key.first);
+      api.push_back(key.second);
+      for (int s : entries[key]) aps.push_back(s);
+      apo.push_back((int)aps.size());
+    }
+    if ((rc = dev_upload(c, &L.pk_block, pkb))) return rc;
+    if ((rc = dev_upload(c, &L.pk_idx, pki))) return rc;
+    L.n_pack = (int)pkb.size();
+    if ((rc = dev_alloc(c, &L.pack, (size_t)L.n_pack * 5))) return rc;
+    if ((rc = dev_upload(c, &L.ap_block, apb))) return rc;
+    if ((rc = dev_upload(c, &L.ap_idx, api))) return rc;
+    if ((rc = dev_upload(c, &L.ap_off, apo))) return rc;
+    if ((rc = dev_upload(c, &L.ap_slot, aps))) return rc;
+    L.n_ap = (int)apb.size();
+  }
+
+  if ((rc = dev_alloc(c, &L.partials, (size_t)L.n_int_chunks))) return rc;
+  if ((rc = dev_alloc(c, &L.hist, (size_t)kHistCap))) return rc;
+  if ((rc = dev_alloc(c, &L.counter, 1))) return rc;
+  if ((rc = dev_alloc(c, &L.dtmin, 1))) return rc;
+  return 0;
+}
+
+// --------------------------------------------------------------------------
+// stage launchers (templated on storage S and compute T)
+// --------------------------------------------------------------------------
+template <typename S, typename T>
+struct Stages {
+  static const BlockDev<S>* blocks(orion_case_t c) { return static_cast<const BlockDev<S>*>(c->d_blocks); }
+
+  // Line kernels take up to kLineSmemBudget of dynamic shared memory; the
+  // attribute is set once, before any stream capture.
+  static int set_attributes() {
+    const int b = (int)kLineSmemBudget;
+    CUDA_TRY(cudaFuncSetAttribute(k_viscous<0, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CUDA_TRY(cudaFuncSetAttribute(k_viscous<1, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CUDA_TRY(cudaFuncSetAttribute(k_viscous<2, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CUDA_TRY(cudaFuncSetAttribute(k_inviscid<0, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CUDA_TRY(cudaFuncSetAttribute(k_inviscid<1, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CUDA_TRY(cudaFuncSetAttribute(k_inviscid<2, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    return 0;
+  }
+
+  static int exchange(orion_case_t c) {
+    auto& L = c->L;
+    if (L.n_halo > 0)
+      k_halo_copy<<<(L.n_halo + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(
+          static_cast<double*>(c->arena), L.halo_src, L.halo_dst, L.n_halo);
+    return 0;
+  }
+
+  static int bc(orion_case_t c) {
+    auto& L = c->L;
+    for (size_t p = 0; p + 1 < L.phase_off.size(); ++p) {
+      const int nr = L.phase_off[p + 1] - L.phase_off[p];
+      if (nr <= 0 || L.phase_maxpts[p] <= 0) continue;
+      dim3 grid((L.phase_maxpts[p] + kThreads - 1) / kThreads, nr);
+      k_bc_phase<S><<<grid, kThreads, 0, c->stream>>>(blocks(c), L.regions, L.phase_regions + L.phase_off[p], c->P);
+    }
+    return 0;
+  }
+
+  static int state(orion_case_t c, bool with_dt, bool with_q) {
+    auto& L = c->L;
+    if (with_dt) k_step_begin<<<1, 32, 0, c->stream>>>(L.dtmin);
+    if (with_dt && with_q)
+      k_state<S, true, true><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dtmin);
+    else if (with_dt)
+      k_state<S, false, true><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dtmin);
+    else if (with_q)
+      k_state<S, true, false><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dtmin);
+    else
+      k_state<S, false, false><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dtmin);
+    return 0;
+  }
+
+  static int timestep(orion_case_t c) {
+    auto& L = c->L;
+    k_step_begin<<<1, 32, 0, c->stream>>>(L.dtmin);
+    k_timestep<S><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P, L.dtmin);
+    return 0;
+  }
+
+  template <int D>
+  static void visc_dir(orion_case_t c) {
+    auto& L = c->L;
+    const size_t smem = (size_t)L.lanes[D] * (L.lmax[D] + 1) * 4 * sizeof(T);
+    k_viscous<D, S, T><<<L.n_tiles[D], kThreads, smem, c->stream>>>(blocks(c), L.tiles[D], c->P);
+  }
+
+  static int viscous(orion_case_t c) {
+    if (c->P.nvis != 1) return 0;
+    auto& L = c->L;
+    k_node_derivs<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks);
+    visc_dir<0>(c);
+    visc_dir<1>(c);
+    visc_dir<2>(c);
+    return 0;
+  }
+
+  template <int D>
+  static void inv_dir(orion_case_t c) {
+    auto& L = c->L;
+    const size_t smem = (size_t)L.lanes[D] * (L.lmax[D] + 1) * 5 * sizeof(T);
+    k_inviscid<D, S, T><<<L.n_tiles[D], kThreads, smem, c->stream>>>(blocks(c), L.tiles[D], c->P);
+  }
+
+  static int inviscid(orion_case_t c) {
+    inv_dir<0>(c);
+    inv_dir<1>(c);
+    inv_dir<2>(c);
+    return 0;
+  }
+
+  static int average(orion_case_t c) {
+    auto& L = c->L;
+    if (L.n_pack == 0) return 0;
+    k_iface_pack<S><<<(L.n_pack + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(blocks(c), L.pk_block, L.pk_idx,
+                                                                                       L.pack, L.n_pack);
+    k_iface_apply<S><<<(L.n_ap + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(
+        blocks(c), L.ap_block, L.ap_idx, L.ap_off, L.ap_slot, L.pack, L.n_ap);
+    return 0;
+  }
+
+  static int update(orion_case_t c, bool fuse_residual) {
+    auto& L = c->L;
+    k_lusgs_prep<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
+    const int np = L.max_planes;
+    for (int s = 0; s < np; ++s)
+      k_sweep_plane<S, T, SW_LUSGS_FWD><<<L.n_plane_chunks, kThreads, 0, c->stream>>>(blocks(c), L.plane_chunks, c->P, s, 0);
+    for (int s = 0; s < np; ++s)
+      k_sweep_plane<S, T, SW_LUSGS_BWD><<<L.n_plane_chunks, kThreads, 0, c->stream>>>(blocks(c), L.plane_chunks, c->P, s, 1);
+    for (int s = 0; s < np; ++s)
+      k_sweep_plane<S, T, SW_GS><<<L.n_plane_chunks, kThreads, 0, c->stream>>>(blocks(c), L.plane_chunks, c->P, s, 0);
+    for (int s = 0; s < np; ++s)
+      k_sweep_plane<S, T, SW_GS><<<L.n_plane_chunks, kThreads, 0, c->stream>>>(blocks(c), L.plane_chunks, c->P, s, 1);
+    if (fuse_residual) {
+      k_update_res<S, true, true, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
+                                                                                         L.partials);
+      residual_final(c);
+    } else {
+      k_update_res<S, true, false, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
+                                                                                          L.partials);
+    }
+    return 0;
+  }
+
+  static void residual_final(orion_case_t c) {
+    auto& L = c->L;
+    k_res_final<S><<<1, 1024, 0, c->stream>>>(blocks(c), c->nblocks, L.partials, L.n_int_chunks, c->total_interior * 5,
+                                              L.dtmin, L.hist, L.counter, kHistCap);
+  }
+
+  static int residual(orion_case_t c) {
+    auto& L = c->L;
+    k_update_res<S, false, true, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
+                                                                                        L.partials);
+    residual_final(c);
+    return 0;
+  }
+
+  // One whole step in the order of OrionSolver::solve (OrionSolver.cpp:141-209).
+  static int step(orion_case_t c, bool with_q) {
+    exchange(c);
+    bc(c);
+    state(c, true, with_q);
+    viscous(c);
+    if (c->P.nvis == 1) average(c);
+    inviscid(c);
+    average(c);
+    update(c, true);
+    return 0;
+  }
+
+  static int init_flow(orion_case_t c, uint64_t seed, double amp) {
+    auto& L = c->L;
+    k_init_flow<S><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, L.pad_base, c->P, seed, amp);
+    return 0;
+  }
+};
+
+using Plain = Stages<double, double>;
+using Mixed = Stages<float, float>;
+
+template <typename F1, typename F2>
+int dispatch(orion_case_t c, F1 plain, F2 mixed) {
+  if (!c) return fail(ORION_E_INVALID, "null case");
+  int rc = (c->prec == ORION_PREC_FP64) ? plain() : mixed();
+  if (rc) return rc;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(ORION_E_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+void destroy_case(orion_case_t c) {
+  if (!c) return;
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  for (void* p : c->allocs) cudaFree(p);
+  if (c->arena) cudaFree(c->arena);
+  if (c->d_blocks) cudaFree(c->d_blocks);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int field_info(orion_case_t c, int block, int field, void** dptr, int* ncomp, bool* is_storage) {
+  if (!c || block < 0 || block >= c->nblocks) return fail(ORION_E_INVALID, "bad block index");
+  *is_storage = false;
+  const bool f64 = c->prec == ORION_PREC_FP64;
+  auto pick = [&](auto& bd) -> int {
+    auto& b = bd[block];
+    switch (field) {
+      case ORION_FIELD_PRIM: *dptr = b.prim; *ncomp = 6; return 0;
+      case ORION_FIELD_Q: *dptr = b.q; *ncomp = 5; return 0;
+      case ORION_FIELD_DQ: *dptr = b.dq; *ncomp = 5; *is_storage = true; return 0;
+      case ORION_FIELD_METRICS: *dptr = (void*)b.metrics; *ncomp = 9; return 0;
+      case ORION_FIELD_VOL: *dptr = (void*)b.vol; *ncomp = 1; return 0;
+      case ORION_FIELD_DT: *dptr = b.dt; *ncomp = 1; *is_storage = true; return 0;
+      case ORION_FIELD_C: *dptr = b.c; *ncomp = 1; *is_storage = true; return 0;
+      case ORION_FIELD_MU: *dptr = b.mu; *ncomp = 1; *is_storage = true; return 0;
+      default: return fail(ORION_E_INVALID, "bad field id");
+    }
+  };
+  return f64 ? pick(c->bd64) : pick(c->bd32);
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+const char* orion_last_error(void) { return g_last_error.c_str(); }
+int orion_abi_version(void) { return ORION_GPU_ABI_VERSION; }
+
+int orion_gpu_init(int device) {
+  int n = 0;
+  CUDA_TRY(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return fail(ORION_E_INVALID, "no such CUDA device");
+  CUDA_TRY(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) return fail(ORION_E_UNSUPPORTED, "this library is built for sm_100a (B200)");
+  return 0;
+}
+
+size_t orion_footprint_estimate(int nblocks, const orion_block_desc_t* blocks, int precision) {
+  if (nblocks <= 0 || !blocks) return 0;
+  const size_t ssz = precision == ORION_PREC_FP64 ? 8 : 4;
+  size_t s = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    HostBlock h;
+    h.idim = blocks[b].idim;
+    h.jdim = blocks[b].jdim;
+    h.kdim = blocks[b].kdim;
+    h.nx = h.idim + 2 * NG;
+    h.ny = h.jdim + 2 * NG;
+    h.nz = h.kdim + 2 * NG;
+    h.npad = (long long)h.nx * h.ny * h.nz;
+    s += block_bytes(h, ssz);
+  }
+  return s + (s / 64);  // work lists and buffers are a small fraction
+}
+
+int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion_params_t* params, int precision,
+                      orion_case_t* out) {
+  if (!out || !params) return fail(ORION_E_INVALID, "null argument");
+  *out = nullptr;
+  if (precision != ORION_PREC_FP64 && precision != ORION_PREC_MIXED) return fail(ORION_E_INVALID, "bad precision");
+  int rc = validate_blocks(nblocks, blocks);
+  if (rc) return rc;
+  std::unique_ptr<orion_case_s> c(new orion_case_s());
+  c->nblocks = nblocks;
+  c->prec = precision;
+  CUDA_TRY(cudaGetDevice(&c->device));
+  auto& P = c->P;
+  P.gamma = params->gamma;
+  P.moo = params->moo;
+  P.reynolds = params->reynolds;
+  P.prl = params->prl;
+  P.cfl = params->cfl;
+  P.twall = params->twall;
+  P.tref = params->tref;
+  P.visc = params->visc;
+  P.roo = params->roo;
+  P.uoo = params->uoo;
+  P.voo = params->voo;
+  P.woo = params->woo;
+  P.poo = params->poo;
+  P.too = params->too;
+  P.csrv = (double)params->csrv;
+  P.nvis = params->nvis;
+  P.method = params->method;
+
+  c->hb.resize(nblocks);
+  long long tot = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    auto& h = c->hb[b];
+    h.idim = blocks[b].idim;
+    h.jdim = blocks[b].jdim;
+    h.kdim = blocks[b].kdim;
+    h.nx = h.idim + 2 * NG;
+    h.ny = h.jdim + 2 * NG;
+    h.nz = h.kdim + 2 * NG;
+    h.npad = (long long)h.nx * h.ny * h.nz;
+    const int dims[3] = {h.idim, h.jdim, h.kdim};
+    for (int r = 0; r < blocks[b].nregions; ++r) {
+      HostRegion hr;
+      hr.r = blocks[b].regions[r];
+      classify_region(hr, dims);
+      if (hr.r.bctype < 0 && hr.s_nd == 0) return fail(ORION_E_INVALID, "interface region is not a plane");
+      h.regions.push_back(hr);
+    }
+    tot += (long long)h.idim * h.jdim * h.kdim;
+  }
+  c->total_interior = tot;
+
+  // arena
+  const size_t ssz = precision == ORION_PREC_FP64 ? 8 : 4;
+  std::vector<size_t> boff(nblocks);
+  size_t total = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    boff[b] = total;
+    total += block_bytes(c->hb[b], ssz);
+  }
+  if (cudaMalloc(&c->arena, total) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ORION_E_NOMEM, "device arena of " + std::to_string(total) + " bytes");
+  }
+  c->arena_bytes = total;
+  CUDA_TRY(cudaMemset(c->arena, 0, total));
+  std::vector<long long> prim_off(nblocks);
+  long long ib = 0;
+  if (precision == ORION_PREC_FP64) {
+    c->bd64.resize(nblocks);
+    for (int b = 0; b < nblocks; ++b) {
+      carve_block(static_cast<char*>(c->arena) + boff[b], c->hb[b], c->bd64[b]);
+      c->bd64[b].int_base = ib;
+      ib += (long long)c->hb[b].idim * c->hb[b].jdim * c->hb[b].kdim;
+      prim_off[b] = (c->bd64[b].prim - static_cast<double*>(c->arena));
+    }
+    CUDA_TRY(cudaMalloc(&c->d_blocks, sizeof(BlockDev<double>) * nblocks));
+    CUDA_TRY(cudaMemcpy(c->d_blocks, c->bd64.data(), sizeof(BlockDev<double>) * nblocks, cudaMemcpyHostToDevice));
+  } else {
+    c->bd32.resize(nblocks);
+    for (int b = 0; b < nblocks; ++b) {
+      carve_block(static_cast<char*>(c->arena) + boff[b], c->hb[b], c->bd32[b]);
+      c->bd32[b].int_base = ib;
+      ib += (long long)c->hb[b].idim * c->hb[b].jdim * c->hb[b].kdim;
+      prim_off[b] = (c->bd32[b].prim - static_cast<double*>(c->arena));
+    }
+    CUDA_TRY(cudaMalloc(&c->d_blocks, sizeof(BlockDev<float>) * nblocks));
+    CUDA_TRY(cudaMemcpy(c->d_blocks, c->bd32.data(), sizeof(BlockDev<float>) * nblocks, cudaMemcpyHostToDevice));
+  }
+
+  // physical-BC dq mask (set_boundary_dq_zero windows, StateUpdater.cpp:447-468)
+  for (int b = 0; b < nblocks; ++b) {
+    const auto& h = c->hb[b];
+    std::vector<uint8_t> mask((size_t)h.npad, 0);
+    for (const auto& hr : h.regions) {
+      if (hr.r.bctype <= 0) continue;
+      for (int k = hr.r.s_st[2] - 1 + NG; k <= hr.r.s_ed[2] - 1 + NG; ++k)
+        for (int j = hr.r.s_st[1] - 1 + NG; j <= hr.r.s_ed[1] - 1 + NG; ++j)
+          for (int i = hr.r.s_st[0] - 1 + NG; i <= hr.r.s_ed[0] - 1 + NG; ++i)
+            if (i >= 0 && j >= 0 && k >= 0 && i < h.nx && j < h.ny && k < h.nz)
+              mask[(size_t)i + (size_t)h.nx * ((size_t)j + (size_t)h.ny * k)] = 1;
+    }
+    const uint8_t* dmask = precision == ORION_PREC_FP64 ? c->bd64[b].bcmask : c->bd32[b].bcmask;
+    CUDA_TRY(cudaMemcpy((void*)dmask, mask.data(), mask.size(), cudaMemcpyHostToDevice));
+  }
+
+  if ((rc = build_lists(c.get(), prim_off))) {
+    destroy_case(c.release());
+    return rc;
+  }
+  rc = (precision == ORION_PREC_FP64) ? Plain::set_attributes() : Mixed::set_attributes();
+  if (rc) {
+    destroy_case(c.release());
+    return rc;
+  }
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(ORION_E_CUDA, "cudaStreamCreate");
+  c->own_stream = true;
+  CUDA_TRY(cudaDeviceSynchronize());
+  *out = c.release();
+  return 0;
+}
+
+int orion_case_destroy(orion_case_t c) {
+  if (!c) return 0;
+  cudaStreamSynchronize(c->stream);
+  destroy_case(c);
+  return 0;
+}
+
+int orion_case_set_stream(orion_case_t c, void* stream) {
+  if (!c) return fail(ORION_E_INVALID, "null case");
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  if (stream) {
+    c->stream = static_cast<cudaStream_t>(stream);
+    c->own_stream = false;
+  } else {
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->own_stream = true;
+  }
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return 0;
+}
+
+int orion_case_sync(orion_case_t c) {
+  if (!c) return fail(ORION_E_INVALID, "null case");
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int orion_case_footprint(orion_case_t c, size_t* bytes) {
+  if (!c || !bytes) return fail(ORION_E_INVALID, "null argument");
+  *bytes = c->arena_bytes;
+  return 0;
+}
+
+int orion_case_upload(orion_case_t c, int block, int field, const double* host) {
+  void* d;
+  int nc;
+  bool st;
+  int rc = field_info(c, block, field, &d, &nc, &st);
+  if (rc) return rc;
+  if (!host) return fail(ORION_E_INVALID, "null host pointer");
+  const size_t n = (size_t)c->hb[block].npad * nc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (st && c->prec != ORION_PREC_FP64) {
+    std::vector<float> tmp(n);
+    for (size_t i = 0; i < n; ++i) tmp[i] = (float)host[i];
+    CUDA_TRY(cudaMemcpy(d, tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+  } else {
+    CUDA_TRY(cudaMemcpy(d, host, n * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  return 0;
+}
+
+int orion_case_download(orion_case_t c, int block, int field, double* host) {
+  void* d;
+  int nc;
+  bool st;
+  int rc = field_info(c, block, field, &d, &nc, &st);
+  if (rc) return rc;
+  if (!host) return fail(ORION_E_INVALID, "null host pointer");
+  const size_t n = (size_t)c->hb[block].npad * nc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (st && c->prec != ORION_PREC_FP64) {
+    std::vector<float> tmp(n);
+    CUDA_TRY(cudaMemcpy(tmp.data(), d, n * sizeof(float), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) host[i] = (double)tmp[i];
+  } else {
+    CUDA_TRY(cudaMemcpy(host, d, n * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  return 0;
+}
+
+int orion_case_init_flow(orion_case_t c, uint64_t seed, double amp) {
+  return dispatch(c, [&] { return Plain::init_flow(c, seed, amp); }, [&] { return Mixed::init_flow(c, seed, amp); });
+}
+
+int orion_exchange_bc(orion_case_t c) {
+  return dispatch(c, [&] { return Plain::exchange(c); }, [&] { return Mixed::exchange(c); });
+}
+int orion_apply_physical_bc(orion_case_t c) {
+  return dispatch(c, [&] { return Plain::bc(c); }, [&] { return Mixed::bc(c); });
+}
+int orion_update_flow_states(orion_case_t c) {
+  return dispatch(c, [&] { return Plain::state(c, false, true); }, [&] { return Mixed::state(c, false, true); });
+}
+int orion_calculate_time_step(orion_case_t c) {
+  return dispatch(c, [&] { return Plain::timestep(c); }, [&] { return Mixed::timestep(c); });
+}
+int orion_compute_viscous_rhs(orion_case_t c) {
+  return dispatch(c, [&] { return Plain::viscous(c); }, [&] { return Mixed::viscous(c); });
+}
+int orion_average_interface_residuals(orion_case_t c) {
+  return dispatch(c, [&] { return Plain::average(c); }, [&] { return Mixed::average(c); });
+}
+int orion_compute_inviscid_rhs(orion_case_t c) {
+  return dispatch(c, [&] { return Plain::inviscid(c); }, [&] { return Mixed::inviscid(c); });
+}
+int orion_update_solution(orion_case_t c) {
+  return dispatch(c, [&] { return Plain::update(c, false); }, [&] { return Mixed::update(c, false); });
+}
+
+static int read_hist(orion_case_t c, long long first, int n, orion_residual_t* out) {
+  std::vector<ResidualOut> h(kHistCap);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CUDA_TRY(cudaMemcpy(h.data(), c->L.hist, sizeof(ResidualOut) * kHistCap, cudaMemcpyDeviceToHost));
+  for (int s = 0; s < n; ++s) {
+    const ResidualOut& r = h[(size_t)((first + s) % kHistCap)];
+    out[s].rms = r.rms;
+    out[s].max = r.max;
+    for (int m = 0; m < 5; ++m) out[s].max_loc[m] = r.loc[m];
+    out[s].pad = 0;
+    out[s].phydtime = r.phydtime;
+  }
+  return 0;
+}
+
+int orion_residual_compute(orion_case_t c, orion_residual_t* out) {
+  if (!c || !out) return fail(ORION_E_INVALID, "null argument");
+  int cnt = 0;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CUDA_TRY(cudaMemcpy(&cnt, c->L.counter, sizeof(int), cudaMemcpyDeviceToHost));
+  int rc = dispatch(c, [&] { return Plain::residual(c); }, [&] { return Mixed::residual(c); });
+  if (rc) return rc;
+  return read_hist(c, cnt, 1, out);
+}
+
+int orion_phydtime(orion_case_t c, double* out) {
+  if (!c || !out) return fail(ORION_E_INVALID, "null argument");
+  unsigned long long bits = 0;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CUDA_TRY(cudaMemcpy(&bits, c->L.dtmin, sizeof(bits), cudaMemcpyDeviceToHost));
+  double v;
+  std::memcpy(&v, &bits, sizeof(v));
+  *out = v;
+  return 0;
+}
+
+static int ensure_graph(orion_case_t c) {
+  if (c->graph) return 0;
+  cudaGraph_t g;
+  CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = (c->prec == ORION_PREC_FP64) ? Plain::step(c, true) : Mixed::step(c, false);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(ORION_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&c->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    c->graph = nullptr;
+    return fail(ORION_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  }
+  return 0;
+}
+
+int orion_step_async(orion_case_t c, int nsteps) {
+  if (!c || nsteps < 0) return fail(ORION_E_INVALID, "bad arguments");
+  int rc = ensure_graph(c);
+  if (rc) return rc;
+  for (int s = 0; s < nsteps; ++s) CUDA_TRY(cudaGraphLaunch(c->graph, c->stream));
+  c->steps_done += nsteps;
+  return 0;
+}
+
+int orion_step(orion_case_t c, int nsteps, orion_residual_t* hist) {
+  if (!c || nsteps < 0) return fail(ORION_E_INVALID, "bad arguments");
+  int cnt = 0;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CUDA_TRY(cudaMemcpy(&cnt, c->L.counter, sizeof(int), cudaMemcpyDeviceToHost));
+  int done = 0;
+  while (done < nsteps) {
+    const int n = std::min(nsteps - done, kHistCap);
+    int rc = orion_step_async(c, n);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (hist) {
+      rc = read_hist(c, (long long)cnt + done, n, hist + done);
+      if (rc) return rc;
+    }
+    done += n;
+  }
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int orion_last_residual(orion_case_t c, orion_residual_t* out) {
+  if (!c || !out) return fail(ORION_E_INVALID, "null argument");
+  int cnt = 0;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CUDA_TRY(cudaMemcpy(&cnt, c->L.counter, sizeof(int), cudaMemcpyDeviceToHost));
+  if (cnt <= 0) return fail(ORION_E_INVALID, "no step has run");
+  return read_hist(c, cnt - 1, 1, out);
+}
+
+}  // extern "C"

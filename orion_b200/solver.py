@@ -1,0 +1,305 @@
+"""Host-side mirror of ORION's per-step solver interface over the C ABI.
+
+``FlowFieldSet`` here is a device-resident case (the reference's
+``preprocess::FlowFieldSet``, src/preprocess/FlowField.hpp:73-87, holds host
+arrays; this one holds device arrays and copies on request).  The classes
+below carry the reference's names and static-method signatures
+(src/solver/*.hpp, src/bc/PhysicalBC.hpp) so a driver loop reads the same:
+
+    HaloExchanger().exchange_bc(bc, fs)
+    apply_physical_bc(bc, fs, params)
+    StateUpdater.update_flow_states(fs, params)
+    TimeIntegrator.calculate_time_step(fs, params)
+    FluxComputer.compute_viscous_rhs(fs, params)
+    HaloExchanger().average_interface_residuals(bc, fs)
+    InviscidFluxComputer.compute_inviscid_rhs(fs, params)
+    StateUpdater.update_solution(fs, bc, params)
+    ResidualMonitor.compute(fs, params) -> ResidualStats
+
+Errors raise ``OrionError`` (the reference throws std::runtime_error or exits).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import OrionError, check
+from .cases import NG, Case, FlowParams, splitmix64_uniform
+
+
+@dataclass
+class ResidualStats:
+    """ResidualStats (src/solver/ResidualMonitor.hpp:8-12) plus phydtime."""
+    rms_residual: float
+    max_residual: float
+    max_loc: tuple
+    phydtime: float
+
+
+def _params_struct(p: FlowParams) -> _lib.Params:
+    s = _lib.Params()
+    s.gamma, s.moo, s.reynolds, s.prl = p.gamma, p.moo, p.reynolds, p.prl
+    s.cfl, s.twall, s.tref, s.visc = p.cfl, p.twall, p.tref, p.visc
+    s.roo, s.uoo, s.voo, s.woo, s.poo, s.too = p.roo, p.uoo, p.voo, p.woo, p.poo, p.too
+    s.nvis, s.method, s.ntmst, s.csrv = p.nvis, p.method, p.ntmst, p.csrv
+    return s
+
+
+def _block_descs(case: Case):
+    keep = []
+    descs = (_lib.BlockDesc * len(case.blocks))()
+    for n, b in enumerate(case.blocks):
+        regs = (_lib.Region * len(b.regions))()
+        for r, g in enumerate(b.regions):
+            regs[r].s_st[:] = g.s_st
+            regs[r].s_ed[:] = g.s_ed
+            regs[r].bctype = g.bctype
+            regs[r].t_st[:] = g.t_st
+            regs[r].t_ed[:] = g.t_ed
+            regs[r].nbt = g.nbt
+            regs[r].ibcwin = g.ibcwin
+        keep.append(regs)
+        descs[n].idim, descs[n].jdim, descs[n].kdim = b.idim, b.jdim, b.kdim
+        descs[n].nregions = len(b.regions)
+        descs[n].regions = C.cast(regs, C.POINTER(_lib.Region))
+    return descs, keep
+
+
+def grid_metrics(block, gcl: int = 1):
+    """Metrics (9, nz, ny, nx) and vol (nz, ny, nx) of one block, padded, ghosts zero."""
+    lib = _lib.load()
+    nx, ny, nz = block.padded
+    met = np.zeros((9, nz, ny, nx))
+    vol = np.zeros((nz, ny, nx))
+    x = np.ascontiguousarray(block.x, dtype=np.float64)
+    y = np.ascontiguousarray(block.y, dtype=np.float64)
+    z = np.ascontiguousarray(block.z, dtype=np.float64)
+    check(lib.orion_grid_metrics_host(block.idim, block.jdim, block.kdim, x.ctypes.data, y.ctypes.data,
+                                      z.ctypes.data, gcl, met.ctypes.data, vol.ctypes.data))
+    return met, vol
+
+
+def footprint_estimate(case: Case, precision: int = _lib.PREC_FP64) -> int:
+    descs, _keep = _block_descs(case)
+    return int(_lib.load().orion_footprint_estimate(len(case.blocks), descs, precision))
+
+
+class FlowFieldSet:
+    """A device-resident case.  ``precision`` is PREC_FP64 (plain) or PREC_MIXED."""
+
+    def __init__(self, case: Case, precision: int = _lib.PREC_FP64, device: int = 0,
+                 metrics: Optional[Sequence] = None, init: bool = True):
+        lib = _lib.load()
+        check(lib.orion_gpu_init(device))
+        self.case = case
+        self.precision = precision
+        self.params = case.params
+        descs, keep = _block_descs(case)
+        h = C.c_void_p()
+        check(lib.orion_case_create(len(case.blocks), descs, C.byref(_params_struct(case.params)), precision,
+                                    C.byref(h)))
+        self._h = h
+        self._keep = keep
+        if metrics is None:
+            metrics = [grid_metrics(b, case.params.gcl) for b in case.blocks]
+        for n, (met, vol) in enumerate(metrics):
+            self.upload(n, "metrics", met)
+            self.upload(n, "vol", vol)
+        if init:
+            check(lib.orion_case_init_flow(self._h, case.noise_seed, case.noise_amp))
+            self.sync()
+
+    # ------------------------------------------------------------------
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().orion_case_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        check(_lib.load().orion_case_sync(self._h))
+
+    def footprint(self) -> int:
+        v = C.c_size_t()
+        check(_lib.load().orion_case_footprint(self._h, C.byref(v)))
+        return int(v.value)
+
+    def upload(self, block: int, field: str, arr: np.ndarray):
+        fid = _lib.FIELD_NAMES[field]
+        b = self.case.blocks[block]
+        nx, ny, nz = b.padded
+        nc = _lib.FIELD_NCOMP[fid]
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.size != nc * nx * ny * nz:
+            raise OrionError(f"{field}: expected {nc * nx * ny * nz} values, got {a.size}")
+        check(_lib.load().orion_case_upload(self._h, block, fid, a.ctypes.data))
+
+    def download(self, block: int, field: str) -> np.ndarray:
+        fid = _lib.FIELD_NAMES[field]
+        b = self.case.blocks[block]
+        nx, ny, nz = b.padded
+        nc = _lib.FIELD_NCOMP[fid]
+        a = np.empty((nc, nz, ny, nx) if nc > 1 else (nz, ny, nx))
+        check(_lib.load().orion_case_download(self._h, block, fid, a.ctypes.data))
+        return a
+
+    def upload_state(self, state: dict):
+        """Uploads every field of a reference-style state (per block dict of arrays)."""
+        for n, blk in enumerate(state["blocks"]):
+            for name in ("prim", "q", "dq", "metrics", "vol", "dt", "c", "mu"):
+                if name in blk:
+                    self.upload(n, name, blk[name])
+
+    # ------------------------------------------------------------------
+    def step(self, nsteps: int) -> np.ndarray:
+        """Runs nsteps whole steps (graph-captured); returns the residual history
+        as an array (nsteps, 8): rms, max, loc[5], phydtime."""
+        hist = (_lib.Residual * max(nsteps, 1))()
+        check(_lib.load().orion_step(self._h, nsteps, hist))
+        out = np.zeros((nsteps, 8))
+        for s in range(nsteps):
+            r = hist[s]
+            out[s, 0] = r.rms
+            out[s, 1] = r.max
+            out[s, 2:7] = list(r.max_loc)
+            out[s, 7] = r.phydtime
+        return out
+
+    def step_async(self, nsteps: int):
+        check(_lib.load().orion_step_async(self._h, nsteps))
+
+    def last_residual(self) -> ResidualStats:
+        r = _lib.Residual()
+        check(_lib.load().orion_last_residual(self._h, C.byref(r)))
+        return ResidualStats(r.rms, r.max, tuple(r.max_loc), r.phydtime)
+
+    def conservative(self, block: int) -> np.ndarray:
+        """Q from the current prim (update_conservative_block formula,
+        src/solver/StateUpdater.cpp:108-124) at interior points."""
+        prim = self.download(block, "prim")
+        return conservative_from_prim(prim, self.params.gamma)
+
+
+def conservative_from_prim(prim: np.ndarray, gamma: float) -> np.ndarray:
+    rho, u, v, w, p = prim[0], prim[1], prim[2], prim[3], prim[4]
+    rc = np.where(rho < 0.0, np.abs(rho), rho)
+    q = np.empty((5,) + rho.shape)
+    q[0] = rc
+    q[1] = rc * u
+    q[2] = rc * v
+    q[3] = rc * w
+    ke = 0.5 * rc * (u * u + v * v + w * w)
+    q[4] = p * (1.0 / (gamma - 1.0)) + ke
+    return q
+
+
+# ---------------------------------------------------------------------------
+# reference-named facade
+# ---------------------------------------------------------------------------
+class HaloExchanger:
+    """src/solver/HaloExchanger.hpp"""
+
+    def exchange_bc(self, bc, fs: FlowFieldSet):
+        check(_lib.load().orion_exchange_bc(fs.handle))
+
+    def average_interface_residuals(self, bc, fs: FlowFieldSet):
+        check(_lib.load().orion_average_interface_residuals(fs.handle))
+
+
+def apply_physical_bc(bc, fs: FlowFieldSet, params=None):
+    """src/bc/PhysicalBC.hpp:17-19"""
+    check(_lib.load().orion_apply_physical_bc(fs.handle))
+
+
+class StateUpdater:
+    """src/solver/StateUpdater.hpp"""
+
+    @staticmethod
+    def update_flow_states(fs: FlowFieldSet, params=None):
+        check(_lib.load().orion_update_flow_states(fs.handle))
+
+    @staticmethod
+    def update_solution(fs: FlowFieldSet, bc=None, params=None):
+        check(_lib.load().orion_update_solution(fs.handle))
+
+
+class TimeIntegrator:
+    """src/solver/TimeIntegrator.hpp"""
+
+    @staticmethod
+    def calculate_time_step(fs: FlowFieldSet, params=None) -> float:
+        lib = _lib.load()
+        check(lib.orion_calculate_time_step(fs.handle))
+        v = C.c_double()
+        check(lib.orion_phydtime(fs.handle, C.byref(v)))
+        if params is not None and hasattr(params, "phydtime"):
+            params.phydtime = v.value
+        return v.value
+
+
+class FluxComputer:
+    """src/solver/FluxComputer.hpp"""
+
+    @staticmethod
+    def compute_viscous_rhs(fs: FlowFieldSet, params=None):
+        check(_lib.load().orion_compute_viscous_rhs(fs.handle))
+
+
+class InviscidFluxComputer:
+    """src/solver/InviscidFluxComputer.hpp"""
+
+    @staticmethod
+    def compute_inviscid_rhs(fs: FlowFieldSet, params=None):
+        check(_lib.load().orion_compute_inviscid_rhs(fs.handle))
+
+
+class ResidualMonitor:
+    """src/solver/ResidualMonitor.hpp"""
+
+    @staticmethod
+    def compute(fs: FlowFieldSet, params=None) -> ResidualStats:
+        r = _lib.Residual()
+        check(_lib.load().orion_residual_compute(fs.handle, C.byref(r)))
+        return ResidualStats(r.rms, r.max, tuple(r.max_loc), r.phydtime)
+
+
+def initial_prim(case: Case) -> List[np.ndarray]:
+    """Host restatement of the device initial state (freestream + noise + T),
+    used to check orion_case_init_flow."""
+    p = case.params
+    out = []
+    start = 0
+    for b in case.blocks:
+        nx, ny, nz = b.padded
+        n = nx * ny * nz
+        prim = np.zeros((6, nz, ny, nx))
+        prim[0] = p.roo
+        prim[1] = p.uoo
+        prim[2] = p.voo
+        prim[3] = p.woo
+        prim[4] = p.poo
+        if case.noise_amp != 0.0:
+            r = splitmix64_uniform(case.noise_seed, 2 * start, 2 * n).reshape(n, 2)
+            r1 = r[:, 0].reshape(nz, ny, nx)
+            r2 = r[:, 1].reshape(nz, ny, nx)
+            prim[0] = prim[0] * (1.0 + case.noise_amp * (2.0 * r1 - 1.0))
+            prim[1] = prim[1] * (1.0 + case.noise_amp * (2.0 * r2 - 1.0))
+        rho = np.maximum(prim[0], 1.0e-30)
+        a2 = p.gamma * prim[4] / rho
+        prim[5] = (p.moo * p.moo) * a2 if p.nvis == 1 else p.too
+        out.append(prim)
+        start += n
+    return out
