@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 per-step solver path (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config C] [--impl ours|reference]
+
+Workload (default --config 3): bump channel 385x257x129 points (13.3M) in 64
+seeded uneven blocks, Mach 0.8, Re 1e5, synthetic initial state (freestream +
+1% seeded noise).  A step is one full solver time step of the whole case.
+`value` is the mixed-precision batched path (FP32 flux / viscous / LU-SGS
+increments, FP64 metrics, Q update and norms); the plain FP64 path is timed
+beside it and the L2 error of the mixed state against the plain state after
+the same steps is reported.  Every GPU runs its own replica (weak scaling, no
+collective on the data path); times are CUDA events, max over ranks.
+
+--impl reference times the reference's own CPU implementation (compiled from
+its sources into oracle/_ref) on a bounded sample of the same workload: some
+of its blocks, each run as a standalone case by one reference process, all
+processes concurrently on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s/GPU plain vs mixed-batched at ≤1e-6 L2 err; p50/p99 solve ms"
+UNIT = "cell-updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+# Algorithmic bytes per grid point of each stage (each stage reads its inputs
+# and writes its outputs once): (plain FP64, mixed).
+STAGE_BYTES = {
+    "state": (144, 112), "timestep": (136, 124), "viscous": (200, 152), "inviscid": (192, 152),
+    "update_solution": (1184, 892), "residual": (56, 32),
+}
+STEP_BYTES = (1912, 1444)
+
+
+def hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks sampler
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 7:
+                continue
+            try:
+                sm.append(float(p[0]))
+                smax = float(p[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# reference CPU measurement (oracle/_ref harness)
+# ---------------------------------------------------------------------------
+def standalone_block_case(case, b):
+    """One block of `case` as its own case: interface faces closed with
+    zero-gradient extrapolation (type 6), physical BCs kept."""
+    from orion_b200 import cases as C
+    blk = case.blocks[b]
+    nb = C.Block(blk.idim, blk.jdim, blk.kdim, blk.x, blk.y, blk.z, [])
+    for r in blk.regions:
+        if r.bctype < 0:
+            nb.regions.append(C.Region(r.s_st, r.s_ed, C.BC_EXTRAPOLATION))
+        else:
+            nb.regions.append(C.Region(r.s_st, r.s_ed, r.bctype))
+    return C.Case(f"{case.name}_blk{b}", [nb], case.params, case.noise_seed, case.noise_amp, 1)
+
+
+def reference_sample(case, steps: int, warmup: int, procs: int):
+    harness = os.path.join(ROOT, "oracle", "_ref", "orion_ref_harness")
+    if not os.path.exists(harness):
+        return None, "reference build oracle/_ref missing"
+    nblk = len(case.blocks)
+    procs = max(1, min(procs, nblk))
+    picks = [int(round(i * (nblk - 1) / max(procs - 1, 1))) for i in range(procs)] if procs > 1 else [0]
+    tmp = tempfile.mkdtemp(prefix="orion_refbench_")
+    runs = []
+    for n, b in enumerate(picks):
+        sub = standalone_block_case(case, b)
+        d = os.path.join(tmp, f"c{n}")
+        sub.write_reference_inputs(d)
+        os.makedirs(d + "/out", exist_ok=True)
+        runs.append((d, sub.npoints))
+    ps = [subprocess.Popen([harness, d, str(steps), d + "/out", "--time-only", "--warmup", str(warmup)],
+                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True) for d, _ in runs]
+    secs, pts = [], 0
+    for p, (_, npts) in zip(ps, runs):
+        out, _ = p.communicate()
+        rec = json.loads(out.strip().splitlines()[-1])
+        secs.append(rec["seconds"])
+        pts += npts
+    value = pts * steps / max(secs)
+    sample = (f"{procs} of the {nblk} blocks of {case.name}, each a standalone reference case "
+              f"(interfaces closed by zero-gradient BCs), {steps} timed steps after {warmup} warm-up, "
+              f"{procs} concurrent single-rank processes; {pts} points")
+    return {"value": value, "unit": UNIT, "cores": procs, "kind": "reference", "sample": sample}, None
+
+
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    from orion_b200 import cases
+    case = cases.config(args.config)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        ncpu = os.cpu_count() or 1
+        rec, err = reference_sample(case, args.steps, args.warmup, min(ncpu, len(case.blocks)))
+        if rec is None:
+            print(json.dumps({"impl": "reference", "unavailable": err}))
+            return
+        line = {"impl": "reference", "metric": METRIC, "value": rec["value"], "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": case.name, "points": case.npoints, "blocks": len(case.blocks)},
+                "cpu_baseline": rec,
+                "e2e": {"value": rec["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from orion_b200 import _lib, solver
+    K, W = args.steps, args.warmup
+    npts = case.npoints
+    metrics = [solver.grid_metrics(b, case.params.gcl) for b in case.blocks]
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_steps(fs, nsteps):
+        s = torch.cuda.ExternalStream(fs.stream_ptr())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record(s)
+        fs.step_async(nsteps)
+        e1.record(s)
+        e1.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1))
+
+    clocks = Clocks(local)
+    results = {}
+    states = {}
+    for name, prec in (("mixed", _lib.PREC_MIXED), ("plain", _lib.PREC_FP64)):
+        fs = solver.FlowFieldSet(case, precision=prec, device=local, metrics=metrics)
+        fs.step(W)
+        if name == "mixed":
+            clocks.start()
+        ms = timed_steps(fs, K)
+        results[name] = {"ms": ms, "launches": fs.step_launches(), "fs": fs}
+        states[name] = [fs.download(b, "prim")[:5, 3:-3, 3:-3, 3:-3] for b in range(len(case.blocks))]
+        if name == "plain":
+            clk = clocks.stop()
+    # L2 error of the mixed state against the plain FP64 state after W+K steps
+    num = sum(float(np.sum((m - p) ** 2)) for m, p in zip(states["mixed"], states["plain"]))
+    den = sum(float(np.sum(p ** 2)) for p in states["plain"])
+    l2 = (num / den) ** 0.5
+    per_rank_pts = npts * K
+    mixed_ms, plain_ms = results["mixed"]["ms"], results["plain"]["ms"]
+    value = world * per_rank_pts / (mixed_ms / 1e3)
+    plain_value = world * per_rank_pts / (plain_ms / 1e3)
+
+    # per-stage timing of one step on the mixed case -> dominant stage roofline
+    fsm = results["mixed"]["fs"]
+    s = torch.cuda.ExternalStream(fsm.stream_ptr())
+    stage_ops = [
+        ("exchange_bc", lambda: solver.HaloExchanger().exchange_bc(None, fsm)),
+        ("apply_physical_bc", lambda: solver.apply_physical_bc(None, fsm)),
+        ("state", lambda: solver.StateUpdater.update_flow_states(fsm)),
+        ("timestep", lambda: _lib.check(_lib.load().orion_calculate_time_step(fsm.handle))),
+        ("viscous", lambda: solver.FluxComputer.compute_viscous_rhs(fsm)),
+        ("average", lambda: solver.HaloExchanger().average_interface_residuals(None, fsm)),
+        ("inviscid", lambda: solver.InviscidFluxComputer.compute_inviscid_rhs(fsm)),
+        ("average2", lambda: solver.HaloExchanger().average_interface_residuals(None, fsm)),
+        ("update_solution", lambda: solver.StateUpdater.update_solution(fsm)),
+        ("residual", lambda: solver.ResidualMonitor.compute(fsm)),
+    ]
+    stage_ms = {}
+    for rep in range(3):
+        for nm, fn in stage_ops:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            fn()
+            e1.record(s)
+            e1.synchronize()
+            if rep > 0:
+                stage_ms.setdefault(nm, []).append(e0.elapsed_time(e1))
+    stage_ms = {k: float(np.mean(v)) for k, v in stage_ms.items()}
+    peak, peak_kind = hbm_peak()
+    dom = max((k for k in stage_ms if k in STAGE_BYTES), key=lambda k: stage_ms[k])
+    bpp = STAGE_BYTES[dom][1]
+    achieved = bpp * npts / (stage_ms[dom] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_kind": f"{peak_kind} hbm_gbs",
+                "bytes_per_point": bpp, "points_per_launch": npts}
+    step_gbs = STEP_BYTES[1] * (value / world) / 1e9
+    step_roofline = {"mixed_achieved_gbs": step_gbs, "mixed_frac": step_gbs / peak,
+                     "plain_achieved_gbs": STEP_BYTES[0] * (plain_value / world) / 1e9,
+                     "plain_frac": STEP_BYTES[0] * (plain_value / world) / 1e9 / peak}
+
+    # end to end through the C ABI with host buffers: every step uploads the
+    # state (prim of every block) from pinned host memory, runs the step and
+    # reads back the state and the residual.
+    fse = results["mixed"]["fs"]
+    host_prim = [torch.from_numpy(fse.download(b, "prim")).pin_memory() for b in range(len(case.blocks))]
+    lib = _lib.load()
+    h2d = sum(int(t.numel()) * 8 for t in host_prim)
+    d2h = h2d + 48
+    import ctypes as C
+    res = _lib.Residual()
+    ne = max(2, min(K, 10))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(ne):
+        for b, t in enumerate(host_prim):
+            _lib.check(lib.orion_case_upload(fse.handle, b, _lib.FIELD_PRIM, C.c_void_p(t.data_ptr())))
+        _lib.check(lib.orion_step(fse.handle, 1, C.byref(res)))
+        for b, t in enumerate(host_prim):
+            _lib.check(lib.orion_case_download(fse.handle, b, _lib.FIELD_PRIM, C.c_void_p(t.data_ptr())))
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world * npts * ne / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ncpu = os.cpu_count() or 1
+        cpu, err = reference_sample(case, 1, 0, min(ncpu, len(case.blocks)))
+        if cpu is None:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": err}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": mixed_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64 (mixed)", "data": "synthetic",
+            "config": {"workload": case.name + " mixed-batched", "points": npts, "blocks": len(case.blocks),
+                       "mach": case.params.moo, "reynolds": case.params.reynolds,
+                       "l2_flush": "none needed: working set %.1f GB per GPU > 126 MB L2" %
+                                   (fsm.footprint() / 1e9)},
+            "plain_fp64": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_ms / K, "dtype": "f64"},
+            "mixed_over_plain": plain_ms / mixed_ms,
+            "mixed_vs_plain_rel_l2": l2,
+            "roofline": roofline, "step_roofline": step_roofline,
+            "stage_ms": stage_ms,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": ne},
+            "gpu_launches": results["mixed"]["launches"] * K,
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    for r in results.values():
+        r["fs"].close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -120,6 +120,10 @@ int orion_case_destroy(orion_case_t c);
 /* Optional: run on a caller-provided cudaStream_t (passed as void*); NULL = the case's own stream. */
 int orion_case_set_stream(orion_case_t c, void* stream);
 int orion_case_sync(orion_case_t c);
+/* The cudaStream_t (as void*) the case enqueues on, for timing with events. */
+int orion_case_stream(orion_case_t c, void** stream);
+/* Kernel launches one captured step issues (after the first orion_step). */
+int orion_case_step_launches(orion_case_t c, int* n);
 /* Device bytes held by the case (the HBM footprint used for admission). */
 int orion_case_footprint(orion_case_t c, size_t* bytes);
 size_t orion_footprint_estimate(int nblocks, const orion_block_desc_t* blocks, int precision);

@@ -10,12 +10,12 @@
 // viscous RHS, so the reference driver itself can never take a second step).
 //
 // Usage:
-//   orion_ref_harness <case_dir> <nsteps> <out_dir> [--snap-step S] [--no-final]
-//                     [--time-only]
+//   orion_ref_harness <case_dir> <nsteps> <out_dir> [--snap-step S] [--time-only]
+//                     [--warmup W]
 // Writes <out_dir>/init.bin, final.bin (field states), hist.bin (residual
 // history) and, with --snap-step S, snap_S_<stage>.bin after every stage of
 // step S.  With --time-only it prints the step-loop wall time and writes
-// nothing but hist.bin.
+// nothing but hist.bin.  --warmup W runs W untimed steps before the timed ones.
 #include <mpi.h>
 
 #include <chrono>
@@ -108,10 +108,12 @@ int main(int argc, char** argv) {
   const std::string out = argv[3];
   int snap_step = -1;
   bool time_only = false;
+  int warmup = 0;
   for (int a = 4; a < argc; ++a) {
     std::string s = argv[a];
     if (s == "--snap-step" && a + 1 < argc) snap_step = std::atoi(argv[++a]);
     else if (s == "--time-only") time_only = true;
+    else if (s == "--warmup" && a + 1 < argc) warmup = std::atoi(argv[++a]);
   }
 
   core::Runtime::init(argc, argv);
@@ -168,7 +170,8 @@ int main(int argc, char** argv) {
   };
 
   auto t0 = std::chrono::steady_clock::now();
-  for (int step = 0; step < nsteps; ++step) {
+  for (int step = -warmup; step < nsteps; ++step) {
+    if (step == 0) t0 = std::chrono::steady_clock::now();
     snap(step, "pre");
     halo.exchange_bc(bcd, fs);
     snap(step, "exchange");
@@ -191,6 +194,7 @@ int main(int argc, char** argv) {
     solver::StateUpdater::update_solution(fs, bcd, params);
     snap(step, "update");
     auto rs = solver::ResidualMonitor::compute(fs, params);
+    if (step < 0) continue;
     hist.push_back(rs.rms_residual);
     hist.push_back(rs.max_residual);
     for (int m = 0; m < 5; ++m) hist.push_back((double)rs.max_loc[m]);

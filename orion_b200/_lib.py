@@ -51,6 +51,8 @@ SIGNATURES = {
     "orion_case_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "orion_case_sync": (C.c_int, [C.c_void_p]),
     "orion_case_footprint": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
+    "orion_case_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "orion_case_step_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "orion_footprint_estimate": (C.c_size_t, [C.c_int, C.POINTER(BlockDesc), C.c_int]),
     "orion_case_upload": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "orion_case_download": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),

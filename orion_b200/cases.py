@@ -219,7 +219,7 @@ def uneven_splits(n: int, parts: int, rng: np.random.Generator, ratio: float = 3
         ext = np.maximum(np.round(w).astype(int), MIN_BLOCK_DIM - 1)
         ext[-1] = cells - ext[:-1].sum()
         if ext.min() >= MIN_BLOCK_DIM - 1 and ext.max() <= ratio * ext.min() + 1:
-            return [0] + list(np.cumsum(ext))
+            return [0] + [int(v) for v in np.cumsum(ext)]
     return even_splits(n, parts)
 
 

@@ -94,6 +94,7 @@ struct orion_case_s {
   long long total_interior = 0;
   cudaGraphExec_t graph = nullptr;
   long long steps_done = 0;
+  int step_launches = 0;
 };
 
 namespace {
@@ -654,6 +655,27 @@ int field_info(orion_case_t c, int block, int field, void** dptr, int* ncomp, bo
 // ============================================================================
 // C ABI
 // ============================================================================
+static int ensure_graph(orion_case_t c) {
+  if (c->graph) return 0;
+  cudaGraph_t g;
+  CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = (c->prec == ORION_PREC_FP64) ? Plain::step(c, true) : Mixed::step(c, false);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(ORION_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  size_t nodes = 0;
+  cudaGraphGetNodes(g, nullptr, &nodes);
+  c->step_launches = (int)nodes;
+  e = cudaGraphInstantiate(&c->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    c->graph = nullptr;
+    return fail(ORION_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  }
+  return 0;
+}
+
+
 extern "C" {
 
 const char* orion_last_error(void) { return g_last_error.c_str(); }
@@ -843,6 +865,20 @@ int orion_case_sync(orion_case_t c) {
   return 0;
 }
 
+int orion_case_stream(orion_case_t c, void** stream) {
+  if (!c || !stream) return fail(ORION_E_INVALID, "null argument");
+  *stream = (void*)c->stream;
+  return 0;
+}
+
+int orion_case_step_launches(orion_case_t c, int* n) {
+  if (!c || !n) return fail(ORION_E_INVALID, "null argument");
+  int rc = ensure_graph(c);
+  if (rc) return rc;
+  *n = c->step_launches;
+  return 0;
+}
+
 int orion_case_footprint(orion_case_t c, size_t* bytes) {
   if (!c || !bytes) return fail(ORION_E_INVALID, "null argument");
   *bytes = c->arena_bytes;
@@ -949,23 +985,6 @@ int orion_phydtime(orion_case_t c, double* out) {
   double v;
   std::memcpy(&v, &bits, sizeof(v));
   *out = v;
-  return 0;
-}
-
-static int ensure_graph(orion_case_t c) {
-  if (c->graph) return 0;
-  cudaGraph_t g;
-  CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = (c->prec == ORION_PREC_FP64) ? Plain::step(c, true) : Mixed::step(c, false);
-  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-  if (rc) return rc;
-  if (e != cudaSuccess) return fail(ORION_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-  e = cudaGraphInstantiate(&c->graph, g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) {
-    c->graph = nullptr;
-    return fail(ORION_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-  }
   return 0;
 }
 

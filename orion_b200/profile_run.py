@@ -1,0 +1,34 @@
+"""Runs a configuration for a few steps, for profilers (ncu launch lists and
+single-kernel captures).
+
+    python -m orion_b200.profile_run --config 1 --steps 2 --warmup 1 --precision mixed
+"""
+from __future__ import annotations
+
+import argparse
+
+from . import _lib, cases, solver
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--config", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "plain"])
+    ap.add_argument("--small", action="store_true", help="a 2x2x2-block 97x65x49 case instead")
+    a = ap.parse_args()
+    if a.small:
+        case = cases.bump_case("profile_small", 97, 65, 49, split=(2, 2, 2), nsteps=a.steps)
+    else:
+        case = cases.config(a.config)
+    prec = _lib.PREC_MIXED if a.precision == "mixed" else _lib.PREC_FP64
+    fs = solver.FlowFieldSet(case, precision=prec)
+    fs.step(a.warmup)
+    h = fs.step(a.steps)
+    print(f"{case.name} {a.precision}: {a.steps} steps, rms {h[-1, 0]:.6e}")
+    fs.close()
+
+
+if __name__ == "__main__":
+    main()

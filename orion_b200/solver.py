@@ -132,6 +132,16 @@ class FlowFieldSet:
     def sync(self):
         check(_lib.load().orion_case_sync(self._h))
 
+    def stream_ptr(self) -> int:
+        v = C.c_void_p()
+        check(_lib.load().orion_case_stream(self._h, C.byref(v)))
+        return int(v.value or 0)
+
+    def step_launches(self) -> int:
+        v = C.c_int()
+        check(_lib.load().orion_case_step_launches(self._h, C.byref(v)))
+        return int(v.value)
+
     def footprint(self) -> int:
         v = C.c_size_t()
         check(_lib.load().orion_case_footprint(self._h, C.byref(v)))

@@ -1,0 +1,68 @@
+"""Generates the golden fixtures of this directory by running the reference
+solver (compiled from its own sources into oracle/_ref by oracle/Makefile) on
+small seeded cases.
+
+    make -C oracle ref && python tests/golden/gen_golden.py
+
+Each fixture holds the case recipe, the reference's residual history
+(rms, max, max location, phydtime per step) and its final primitive state:
+the full interior state for the single-block case, every 7th interior point
+(flattened, blocks in order) for the multi-block case to keep the file small.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import refio  # noqa: E402
+from orion_b200 import cases  # noqa: E402
+
+NG = 3
+
+RECIPES = {
+    "small_1blk": dict(name="small_1blk", dims=(17, 13, 12), split=(1, 1, 1), nsteps=20, noise_seed=11),
+    "small_8blk": dict(name="small_8blk", dims=(33, 25, 23), split=(2, 2, 2), nsteps=10, noise_seed=12),
+    "small_uneven": dict(name="small_uneven", dims=(41, 27, 25), split=(3, 2, 2), nsteps=8, noise_seed=13,
+                         uneven_seed=5, moo=0.7, reynolds=1.0e4),
+}
+
+
+def build(recipe: dict) -> cases.Case:
+    r = dict(recipe)
+    return cases.small_case(**r)
+
+
+def interior_prim(state, sub: int = 1) -> np.ndarray:
+    parts = []
+    for b in state["blocks"]:
+        p = b["prim"][:5, NG:-NG, NG:-NG, NG:-NG]
+        parts.append(p.reshape(5, -1))
+    flat = np.concatenate(parts, axis=1)
+    return flat[:, ::sub]
+
+
+def main():
+    for key, recipe in RECIPES.items():
+        case = build(recipe)
+        tmp = tempfile.mkdtemp(prefix="golden_")
+        case.write_reference_inputs(os.path.join(tmp, "case"))
+        refio.run_reference(os.path.join(tmp, "case"), case.nsteps, os.path.join(tmp, "out"))
+        hist = refio.read_hist(os.path.join(tmp, "out", "hist.bin"))
+        final = refio.read_state(os.path.join(tmp, "out", "final.bin"))
+        sub = 1 if len(case.blocks) == 1 else 7
+        np.savez_compressed(os.path.join(HERE, key + ".npz"), hist=hist, prim=interior_prim(final, sub),
+                            sub=np.array([sub]), recipe=np.array([json.dumps(recipe)]))
+        print(key, case.npoints, "points", case.nsteps, "steps", hist[-1, :2])
+
+
+if __name__ == "__main__":
+    main()
