@@ -20,14 +20,28 @@ struct BlockDev {
   S* dt;
   S* c;
   S* mu;
-  S* rhs;                 // 5 comps, copy of the masked RHS for the sweeps
-  S* coed;                // LU-SGS diagonal coefficient
   S* duvwt;               // 12 comps: node derivatives of u,v,w,T along xi,eta,zeta
   const uint8_t* bcmask;  // 1 where a physical-BC window zeroes dq
   int ni, nj, nk;         // interior points
   int nx, ny, nz;         // padded
   long long npad;
   long long int_base;     // interior points of all earlier blocks (residual location key)
+
+  // Plane-major ("skewed") copies of the implicit sweeps' operands.  Interior
+  // points are ordered by hyperplane s = ii+jj+kk, then kk, then jj, so each
+  // hyperplane is one contiguous range and a point's face neighbours lie in the
+  // adjacent hyperplanes at offsets given by koff.  Component stride ncomp.
+  int nplanes;            // ni + nj + nk - 2
+  long long ncomp;        // ni * nj * nk
+  const int* koff;        // start of run (s, kk) at koff[s * nk + kk]; koff[nplanes * nk] = ncomp
+  const int* sk_nat;      // padded natural index of each compact point
+  S* sk_metrics;          // 9 comps (static)
+  S* sk_vol;              // static
+  S* sk_prim;             // 5 comps
+  S* sk_mu;
+  S* sk_coed;             // diagonal coefficient
+  S* sk_rhs;              // 5 comps: masked RHS
+  S* sk_dq;               // 5 comps: the increment being swept
 };
 
 // Scalar parameters (orion_params_t after conversion).

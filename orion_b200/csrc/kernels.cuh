@@ -46,7 +46,7 @@ __device__ __forceinline__ long long line_origin(const BlockDev<S>& B, int d, in
 // src/solver/HaloExchanger.cpp:70-179).  The host flattened the pack/unpack
 // order into (src, dst) element offsets, last writer kept.
 // ===========================================================================
-__global__ void k_halo_copy(double* __restrict__ arena, const long long* __restrict__ src,
+static __global__ void k_halo_copy(double* __restrict__ arena, const long long* __restrict__ src,
                             const long long* __restrict__ dst, int n) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) arena[dst[t]] = arena[src[t]];
@@ -423,7 +423,7 @@ __global__ void k_timestep(const BlockDev<S>* __restrict__ blocks, const Chunk* 
   atomic_min_pos_double(dtmin_bits, local_min);
 }
 
-__global__ void k_step_begin(unsigned long long* dtmin_bits) {
+static __global__ void k_step_begin(unsigned long long* dtmin_bits) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *dtmin_bits = (unsigned long long)__double_as_longlong(1000.0);
 }
 
@@ -954,64 +954,100 @@ __global__ void k_iface_apply(const BlockDev<S>* __restrict__ blocks, const int*
 
 // ===========================================================================
 // LU-SGS / symmetric Gauss-Seidel (StateUpdater::update_solution,
-// src/solver/StateUpdater.cpp:267-580).
+// src/solver/StateUpdater.cpp:267-580) on the plane-major layout.
+// Any order that visits a point after its lower face neighbours and before its
+// upper ones reproduces the lexicographic sweeps exactly; the hyperplane order
+// does, and each hyperplane is a contiguous, coalesced range here.
 // ===========================================================================
-// Prep: rhs = dq with physical-BC windows zeroed (set_boundary_dq_zero + the
-// AoS copy), and the diagonal coefficient 1/(1/dt + sum of radii)
-// (get_diag_coeff :267-295), which is the same in all four sweeps.
+template <typename S>
+__device__ __forceinline__ int jlo_of(const BlockDev<S>& B, int s, int kk) {
+  const int v = s - kk - (B.ni - 1);
+  return v > 0 ? v : 0;
+}
+
+template <typename S>
+__device__ __forceinline__ void decode_nat(const BlockDev<S>& B, int nat, int& ii, int& jj, int& kk) {
+  const int i = nat % B.nx;
+  const int r = nat / B.nx;
+  ii = i - NG;
+  jj = r % B.ny - NG;
+  kk = r / B.ny - NG;
+}
+
+// Static skewed operands (metrics, vol): refreshed whenever they are uploaded.
+template <typename S>
+__global__ void k_skew_static(const BlockDev<S>* __restrict__ blocks, int b) {
+  const BlockDev<S> B = blocks[b];
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < B.ncomp; c += (long long)gridDim.x * blockDim.x) {
+    const int nat = B.sk_nat[c];
+    for (int m = 0; m < 9; ++m) B.sk_metrics[m * B.ncomp + c] = (S)B.metrics[m * B.npad + nat];
+    B.sk_vol[c] = (S)B.vol[nat];
+  }
+}
+
+// Prep: gather prim, mu into the skewed layout; rhs = dq with physical-BC
+// windows zeroed (set_boundary_dq_zero + the AoS copy, StateUpdater.cpp:447-570);
+// diagonal coefficient 1/(1/dt + sum of radii) (get_diag_coeff :267-295), the
+// same in all four sweeps.
 template <typename S, typename T>
 __global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const long long np = B.npad;
+  const long long np = B.npad, nc = B.ncomp;
   const T gamma = T(P.gamma), reynolds = T(P.reynolds);
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-    const long long n = ch.start + t;
-    const int ii = (int)(n % B.ni), jj = (int)((n / B.ni) % B.nj), kk = (int)(n / ((long long)B.ni * B.nj));
-    const long long idx = lin(B, NG + ii, NG + jj, NG + kk);
-    const bool masked = B.bcmask[idx] != 0;
-    for (int m = 0; m < 5; ++m) B.rhs[m * np + idx] = masked ? (S)0 : B.dq[m * np + idx];
-    const T rho = (T)B.prim[idx], u = (T)B.prim[np + idx], v = (T)B.prim[2 * np + idx], w = (T)B.prim[3 * np + idx],
-            p = (T)B.prim[4 * np + idx];
+    const long long c = ch.start + t;
+    const int nat = B.sk_nat[c];
+    const bool masked = B.bcmask[nat] != 0;
+    for (int m = 0; m < 5; ++m) B.sk_rhs[m * nc + c] = masked ? (S)0 : B.dq[m * np + nat];
+    const T rho = (T)B.prim[nat], u = (T)B.prim[np + nat], v = (T)B.prim[2 * np + nat],
+            w = (T)B.prim[3 * np + nat], p = (T)B.prim[4 * np + nat];
+    B.sk_prim[c] = (S)rho;
+    B.sk_prim[nc + c] = (S)u;
+    B.sk_prim[2 * nc + c] = (S)v;
+    B.sk_prim[3 * nc + c] = (S)w;
+    B.sk_prim[4 * nc + c] = (S)p;
     T km[9];
-    for (int m = 0; m < 9; ++m) km[m] = (T)B.metrics[m * np + idx];
+    for (int m = 0; m < 9; ++m) km[m] = (T)B.sk_metrics[m * nc + c];
     const T ra = spectral_radius<T>(rho, u, v, w, p, gamma, km[0], km[1], km[2]);
     const T rb = spectral_radius<T>(rho, u, v, w, p, gamma, km[3], km[4], km[5]);
     const T rc = spectral_radius<T>(rho, u, v, w, p, gamma, km[6], km[7], km[8]);
     T rva = T(0), rvb = T(0), rvc = T(0);
+    const T mu = (T)B.mu[nat];
+    B.sk_mu[c] = (S)mu;
     if (P.nvis == 1) {
-      const T mu = (T)B.mu[idx];
-      T vol = (T)B.vol[idx];
+      T vol = (T)B.sk_vol[c];
       if (vol < T(1e-30)) vol = T(1e-30);
       rva = visc_spectral_radius<T>(rho, mu, vol, reynolds, km[0], km[1], km[2]);
       rvb = visc_spectral_radius<T>(rho, mu, vol, reynolds, km[3], km[4], km[5]);
       rvc = visc_spectral_radius<T>(rho, mu, vol, reynolds, km[6], km[7], km[8]);
     }
     const T rad_sum = ra + rb + rc + rva + rvb + rvc;
-    const T term = (T(1) / (T)B.dt[idx]) + rad_sum;
-    B.coed[idx] = (S)(T(1) / term);
+    const T term = (T(1) / (T)B.dt[nat]) + rad_sum;
+    B.sk_coed[c] = (S)(T(1) / term);
   }
 }
 
 enum SweepMode { SW_LUSGS_FWD = 0, SW_LUSGS_BWD = 1, SW_GS = 2 };
 
-// Neighbour contribution (add_nb / add_nb_contrib, StateUpdater.cpp:326-347, 401-426).
+// Neighbour contribution (add_nb / add_nb_contrib, StateUpdater.cpp:326-347, 401-426);
+// cn is the neighbour's compact index, km the current point's metrics for its direction.
 template <typename S, typename T, int MODE>
-__device__ __forceinline__ void sweep_nb(const BlockDev<S>& B, const ParamsDev& P, long long nidx, const T km[3],
+__device__ __forceinline__ void sweep_nb(const BlockDev<S>& B, const ParamsDev& P, long long cn, const T km[3],
                                          T sgn, T rhs0[5]) {
-  const long long np = B.npad;
+  const long long nc = B.ncomp;
   T pn[5], dn[5];
   for (int m = 0; m < 5; ++m) {
-    pn[m] = (T)B.prim[m * np + nidx];
-    dn[m] = (T)B.dq[m * np + nidx];
+    pn[m] = (T)B.sk_prim[m * nc + cn];
+    dn[m] = (T)B.sk_dq[m * nc + cn];
   }
   const T gamma = T(P.gamma);
   const T r = spectral_radius<T>(pn[0], pn[1], pn[2], pn[3], pn[4], gamma, km[0], km[1], km[2]);
   T fs[5];
   flux_split<T>(pn, dn, km[0], km[1], km[2], r, sgn, gamma, fs);
   if (P.nvis == 1) {
-    const T mu_nb = (T)B.mu[nidx];
-    T vol_nb = (T)B.vol[nidx];
+    const T mu_nb = (T)B.sk_mu[cn];
+    T vol_nb = (T)B.sk_vol[cn];
     if (vol_nb < T(1e-30)) vol_nb = T(1e-30);
     const T rv = visc_spectral_radius<T>(pn[0], mu_nb, vol_nb, T(P.reynolds), km[0], km[1], km[2]);
     if (MODE == SW_GS) {
@@ -1028,54 +1064,106 @@ __device__ __forceinline__ void sweep_nb(const BlockDev<S>& B, const ParamsDev& 
 }
 
 template <typename S, typename T, int MODE>
-__device__ __forceinline__ void sweep_point(const BlockDev<S>& B, const ParamsDev& P, int ii, int jj, int kk) {
-  const long long np = B.npad;
-  const long long idx = lin(B, NG + ii, NG + jj, NG + kk);
-  const long long sj = B.nx, sk = (long long)B.nx * B.ny;
+__device__ __forceinline__ void sweep_point(const BlockDev<S>& B, const ParamsDev& P, long long c) {
+  const long long nc = B.ncomp;
+  int ii, jj, kk;
+  decode_nat(B, B.sk_nat[c], ii, jj, kk);
+  const int s = ii + jj + kk;
+  const int nk = B.nk;
   T km[9];
-  for (int m = 0; m < 9; ++m) km[m] = (T)B.metrics[m * np + idx];
+  for (int m = 0; m < 9; ++m) km[m] = (T)B.sk_metrics[m * nc + c];
   T rhs0[5] = {T(0), T(0), T(0), T(0), T(0)};
   if (MODE == SW_LUSGS_FWD || MODE == SW_GS) {
-    if (ii > 0) sweep_nb<S, T, MODE>(B, P, idx - 1, km + 0, T(1), rhs0);
-    if (jj > 0) sweep_nb<S, T, MODE>(B, P, idx - sj, km + 3, T(1), rhs0);
-    if (kk > 0) sweep_nb<S, T, MODE>(B, P, idx - sk, km + 6, T(1), rhs0);
+    const int* ko = B.koff + (s - 1) * nk;
+    if (ii > 0) sweep_nb<S, T, MODE>(B, P, ko[kk] + (jj - jlo_of(B, s - 1, kk)), km + 0, T(1), rhs0);
+    if (jj > 0) sweep_nb<S, T, MODE>(B, P, ko[kk] + (jj - 1 - jlo_of(B, s - 1, kk)), km + 3, T(1), rhs0);
+    if (kk > 0) sweep_nb<S, T, MODE>(B, P, ko[kk - 1] + (jj - jlo_of(B, s - 1, kk - 1)), km + 6, T(1), rhs0);
   }
   if (MODE == SW_LUSGS_BWD || MODE == SW_GS) {
-    if (ii < B.ni - 1) sweep_nb<S, T, MODE>(B, P, idx + 1, km + 0, T(-1), rhs0);
-    if (jj < B.nj - 1) sweep_nb<S, T, MODE>(B, P, idx + sj, km + 3, T(-1), rhs0);
-    if (kk < B.nk - 1) sweep_nb<S, T, MODE>(B, P, idx + sk, km + 6, T(-1), rhs0);
+    const int* ko = B.koff + (s + 1) * nk;
+    if (ii < B.ni - 1) sweep_nb<S, T, MODE>(B, P, ko[kk] + (jj - jlo_of(B, s + 1, kk)), km + 0, T(-1), rhs0);
+    if (jj < B.nj - 1) sweep_nb<S, T, MODE>(B, P, ko[kk] + (jj + 1 - jlo_of(B, s + 1, kk)), km + 3, T(-1), rhs0);
+    if (kk < B.nk - 1) sweep_nb<S, T, MODE>(B, P, ko[kk + 1] + (jj - jlo_of(B, s + 1, kk + 1)), km + 6, T(-1), rhs0);
   }
-  const T coed = (T)B.coed[idx];
+  const T coed = (T)B.sk_coed[c];
   for (int m = 0; m < 5; ++m) {
-    S* d = B.dq + m * np + idx;
+    S* d = B.sk_dq + m * nc + c;
     if (MODE == SW_LUSGS_FWD) {
-      const T explicit_term = -(T)B.rhs[m * np + idx];
+      const T explicit_term = -(T)B.sk_rhs[m * nc + c];
       *d = (S)((explicit_term + rhs0[m]) * coed);
     } else if (MODE == SW_LUSGS_BWD) {
       *d = (S)((T)*d - rhs0[m] * coed);
     } else {
-      const T resid = -(T)B.rhs[m * np + idx];
+      const T resid = -(T)B.sk_rhs[m * nc + c];
       *d = (S)((rhs0[m] + resid) * coed);
     }
   }
 }
 
-// One i+j+k hyperplane of one sweep for every block: points with ii+jj+kk == s.
+// One hyperplane of one sweep for every block; chunks list contiguous compact ranges.
 template <typename S, typename T, int MODE>
-__global__ void k_sweep_plane(const BlockDev<S>* __restrict__ blocks, const PlaneChunk* __restrict__ chunks, ParamsDev P,
-                              int s_fwd, int backward) {
-  const PlaneChunk ch = chunks[blockIdx.x];
+__global__ void __launch_bounds__(256) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
+                                                     const Chunk* __restrict__ chunks, ParamsDev P) {
+  const Chunk ch = chunks[blockIdx.x];
+  if ((int)threadIdx.x >= ch.count) return;
   const BlockDev<S> B = blocks[ch.block];
-  const int t = threadIdx.x;
-  if (t >= ch.count) return;
-  const int smax = B.ni + B.nj + B.nk - 3;
-  const int s = backward ? (smax - s_fwd) : s_fwd;
-  if (s < 0 || s > smax) return;
-  const int n = ch.start + t;
-  const int jj = n % B.nj, kk = n / B.nj;
-  const int ii = s - jj - kk;
-  if (ii < 0 || ii >= B.ni) return;
-  sweep_point<S, T, MODE>(B, P, ii, jj, kk);
+  sweep_point<S, T, MODE>(B, P, ch.start + threadIdx.x);
+}
+
+// Finish: zero the physical-BC windows (set_boundary_dq_zero), scatter dq to
+// the natural layout, limited update (update_limited) and, when DO_RES, the
+// residual partials (ResidualMonitor::compute).
+template <typename S>
+__device__ __forceinline__ void limited_update(const BlockDev<S>& B, const ParamsDev& P, long long idx,
+                                               const double dq[5]);
+__device__ __forceinline__ void res_combine(double& sum, double& mx, long long& key, double osum, double omx,
+                                            long long okey);
+template <int NT>
+__device__ __forceinline__ void block_reduce_res(double& sum, double& mx, long long& key);
+
+template <typename S, bool DO_RES, int NT>
+__global__ void __launch_bounds__(NT) k_sweep_finish(const BlockDev<S>* __restrict__ blocks,
+                                                     const Chunk* __restrict__ chunks, ParamsDev P,
+                                                     ResPartial* __restrict__ partials) {
+  const Chunk ch = chunks[blockIdx.x];
+  const BlockDev<S> B = blocks[ch.block];
+  const long long np = B.npad, nc = B.ncomp;
+  double sum = 0.0, mx = -1.0;
+  long long key = (long long)0x7fffffffffffffffLL;
+  for (int t = threadIdx.x; t < ch.count; t += NT) {
+    const long long c = ch.start + t;
+    const int nat = B.sk_nat[c];
+    double dq[5];
+    const bool masked = B.bcmask[nat] != 0;
+    for (int m = 0; m < 5; ++m) {
+      const S v = masked ? (S)0 : B.sk_dq[m * nc + c];
+      B.dq[m * np + nat] = v;
+      dq[m] = (double)v;
+    }
+    limited_update(B, P, nat, dq);
+    if (DO_RES) {
+      double vol = B.vol[nat];
+      double dt = (double)B.dt[nat];
+      if (vol < 1e-30) vol = 1e-30;
+      if (dt < 1e-30) dt = 1e-30;
+      const double inv_factor = 1.0 / (dt * vol);
+      int ii, jj, kk;
+      decode_nat(B, nat, ii, jj, kk);
+      const long long kbase = (B.int_base + ii + (long long)B.ni * (jj + (long long)B.nj * kk)) * 5;
+      for (int m = 0; m < 5; ++m) {
+        const double res = fabs(dq[m]) * inv_factor;
+        sum += res * res;
+        if (res > mx || (res == mx && kbase + m < key)) {
+          mx = res;
+          key = kbase + m;
+        }
+      }
+    }
+  }
+  if (DO_RES) {
+    block_reduce_res<NT>(sum, mx, key);
+    if (threadIdx.x == 0) partials[blockIdx.x] = ResPartial{sum, mx, key};
+  }
 }
 
 // ===========================================================================
@@ -1197,7 +1285,7 @@ __global__ void __launch_bounds__(NT) k_update_res(const BlockDev<S>* __restrict
       for (int m = 0; m < 5; ++m) {
         const double res = fabs(dq[m]) * inv_factor;
         sum += res * res;
-        if (res > mx) {
+        if (res > mx || (res == mx && kbase + m < key)) {
           mx = res;
           key = kbase + m;
         }

@@ -48,8 +48,8 @@ struct DeviceLists {
   int n_tiles[3] = {0, 0, 0};
   int lanes[3] = {1, 1, 1};
   int lmax[3] = {0, 0, 0};
-  PlaneChunk* plane_chunks = nullptr;
-  int n_plane_chunks = 0;
+  Chunk* sweep_chunks[2] = {nullptr, nullptr};  // forward / backward hyperplane launches
+  std::vector<int> sweep_off[2];                 // host: chunk range of each launch
   int max_planes = 0;
   long long* halo_src = nullptr;
   long long* halo_dst = nullptr;
@@ -75,6 +75,10 @@ struct DeviceLists {
 };
 
 }  // namespace
+
+namespace orion {
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace orion
 
 struct orion_case_s {
   int nblocks = 0;
@@ -134,10 +138,13 @@ size_t block_bytes(const HostBlock& b, size_t ssz) {
   add(np * ssz);      // dt
   add(np * ssz);      // c
   add(np * ssz);      // mu
-  add(5 * np * ssz);  // rhs
-  add(np * ssz);      // coed
   add(12 * np * ssz); // duvwt
   add(np);            // bcmask
+  const size_t nc = (size_t)b.idim * b.jdim * b.kdim;
+  const size_t npl = (size_t)(b.idim + b.jdim + b.kdim - 2);
+  add((npl * b.kdim + 1) * 4);  // koff
+  add(nc * 4);                  // sk_nat
+  add(27 * nc * ssz);           // sk_metrics 9, sk_vol, sk_prim 5, sk_mu, sk_coed, sk_rhs 5, sk_dq 5
   return align_up(s, 256);
 }
 
@@ -159,10 +166,22 @@ void carve_block(char* base, const HostBlock& b, BlockDev<S>& d) {
   d.dt = reinterpret_cast<S*>(take(np * sizeof(S)));
   d.c = reinterpret_cast<S*>(take(np * sizeof(S)));
   d.mu = reinterpret_cast<S*>(take(np * sizeof(S)));
-  d.rhs = reinterpret_cast<S*>(take(5 * np * sizeof(S)));
-  d.coed = reinterpret_cast<S*>(take(np * sizeof(S)));
   d.duvwt = reinterpret_cast<S*>(take(12 * np * sizeof(S)));
   d.bcmask = reinterpret_cast<uint8_t*>(take(np));
+  const size_t nc = (size_t)b.idim * b.jdim * b.kdim;
+  const int npl = b.idim + b.jdim + b.kdim - 2;
+  d.nplanes = npl;
+  d.ncomp = (long long)nc;
+  d.koff = reinterpret_cast<int*>(take(((size_t)npl * b.kdim + 1) * 4));
+  d.sk_nat = reinterpret_cast<int*>(take(nc * 4));
+  S* sk = reinterpret_cast<S*>(take(27 * nc * sizeof(S)));
+  d.sk_metrics = sk;
+  d.sk_vol = sk + 9 * nc;
+  d.sk_prim = sk + 10 * nc;
+  d.sk_mu = sk + 15 * nc;
+  d.sk_coed = sk + 16 * nc;
+  d.sk_rhs = sk + 17 * nc;
+  d.sk_dq = sk + 22 * nc;
   d.ni = b.idim;
   d.nj = b.jdim;
   d.nk = b.kdim;
@@ -188,6 +207,27 @@ int validate_blocks(int nblocks, const orion_block_desc_t* blocks) {
     }
   }
   return 0;
+}
+
+// Plane-major order of a block's interior points: hyperplane s = ii+jj+kk, then
+// kk, then jj.  koff[s*nk + kk] is the start of the (s, kk) run.
+void plane_major_maps(const HostBlock& h, std::vector<int>& koff, std::vector<int>& nat) {
+  const int ni = h.idim, nj = h.jdim, nk = h.kdim;
+  const int npl = ni + nj + nk - 2;
+  koff.assign((size_t)npl * nk + 1, 0);
+  nat.clear();
+  nat.reserve((size_t)ni * nj * nk);
+  for (int s = 0; s < npl; ++s)
+    for (int kk = 0; kk < nk; ++kk) {
+      koff[(size_t)s * nk + kk] = (int)nat.size();
+      const int jlo = std::max(0, s - kk - (ni - 1));
+      const int jhi = std::min(nj - 1, s - kk);
+      for (int jj = jlo; jj <= jhi; ++jj) {
+        const int ii = s - jj - kk;
+        nat.push_back((ii + NG) + h.nx * ((jj + NG) + h.ny * (kk + NG)));
+      }
+    }
+  koff[(size_t)npl * nk] = (int)nat.size();
 }
 
 // --------------------------------------------------------------------------
@@ -235,17 +275,41 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
     L.n_tiles[d] = (int)tiles.size();
   }
 
-  // wavefront plane chunks: (jj,kk) index space of every block
-  std::vector<PlaneChunk> pcs;
-  L.max_planes = 0;
-  for (int b = 0; b < nb; ++b) {
-    const auto& h = c->hb[b];
-    L.max_planes = std::max(L.max_planes, h.idim + h.jdim + h.kdim - 2);
-    const int n = h.jdim * h.kdim;
-    for (int s = 0; s < n; s += kThreads) pcs.push_back(PlaneChunk{b, s, std::min(kThreads, n - s), 0});
+  // wavefront launches: launch t of the forward sweeps covers hyperplane t of
+  // every block, launch t of the backward sweeps hyperplane nplanes-1-t.
+  {
+    L.max_planes = 0;
+    std::vector<std::vector<int>> koffs(nb);
+    for (int b = 0; b < nb; ++b) {
+      const auto& h = c->hb[b];
+      L.max_planes = std::max(L.max_planes, h.idim + h.jdim + h.kdim - 2);
+      std::vector<int> nat;
+      plane_major_maps(h, koffs[b], nat);
+      const BlockDev<double>* b64 = c->bd64.empty() ? nullptr : &c->bd64[b];
+      const BlockDev<float>* b32 = c->bd32.empty() ? nullptr : &c->bd32[b];
+      void* dk = b64 ? (void*)b64->koff : (void*)b32->koff;
+      void* dn = b64 ? (void*)b64->sk_nat : (void*)b32->sk_nat;
+      CUDA_TRY(cudaMemcpy(dk, koffs[b].data(), koffs[b].size() * 4, cudaMemcpyHostToDevice));
+      CUDA_TRY(cudaMemcpy(dn, nat.data(), nat.size() * 4, cudaMemcpyHostToDevice));
+    }
+    for (int dir = 0; dir < 2; ++dir) {
+      std::vector<Chunk> ch;
+      std::vector<int> off{0};
+      for (int t = 0; t < L.max_planes; ++t) {
+        for (int b = 0; b < nb; ++b) {
+          const auto& h = c->hb[b];
+          const int npl = h.idim + h.jdim + h.kdim - 2;
+          if (t >= npl) continue;
+          const int sp = dir == 0 ? t : npl - 1 - t;
+          const int lo = koffs[b][(size_t)sp * h.kdim], hi = koffs[b][(size_t)(sp + 1) * h.kdim];
+          for (int x = lo; x < hi; x += kThreads) ch.push_back(Chunk{b, std::min(kThreads, hi - x), (long long)x});
+        }
+        off.push_back((int)ch.size());
+      }
+      if ((rc = dev_upload(c, &L.sweep_chunks[dir], ch))) return rc;
+      L.sweep_off[dir] = off;
+    }
   }
-  if ((rc = dev_upload(c, &L.plane_chunks, pcs))) return rc;
-  L.n_plane_chunks = (int)pcs.size();
 
   // ---------------- halo copy (exchange_bc) ----------------
   {
@@ -549,26 +613,36 @@ struct Stages {
     return 0;
   }
 
+  template <int MODE>
+  static void sweep(orion_case_t c, int dir) {
+    auto& L = c->L;
+    const auto& off = L.sweep_off[dir];
+    for (int t = 0; t + 1 < (int)off.size(); ++t) {
+      const int n = off[t + 1] - off[t];
+      if (n > 0) k_sweep_plane<S, T, MODE><<<n, kThreads, 0, c->stream>>>(blocks(c), L.sweep_chunks[dir] + off[t], c->P);
+    }
+  }
+
   static int update(orion_case_t c, bool fuse_residual) {
     auto& L = c->L;
     k_lusgs_prep<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
-    const int np = L.max_planes;
-    for (int s = 0; s < np; ++s)
-      k_sweep_plane<S, T, SW_LUSGS_FWD><<<L.n_plane_chunks, kThreads, 0, c->stream>>>(blocks(c), L.plane_chunks, c->P, s, 0);
-    for (int s = 0; s < np; ++s)
-      k_sweep_plane<S, T, SW_LUSGS_BWD><<<L.n_plane_chunks, kThreads, 0, c->stream>>>(blocks(c), L.plane_chunks, c->P, s, 1);
-    for (int s = 0; s < np; ++s)
-      k_sweep_plane<S, T, SW_GS><<<L.n_plane_chunks, kThreads, 0, c->stream>>>(blocks(c), L.plane_chunks, c->P, s, 0);
-    for (int s = 0; s < np; ++s)
-      k_sweep_plane<S, T, SW_GS><<<L.n_plane_chunks, kThreads, 0, c->stream>>>(blocks(c), L.plane_chunks, c->P, s, 1);
+    sweep<SW_LUSGS_FWD>(c, 0);
+    sweep<SW_LUSGS_BWD>(c, 1);
+    sweep<SW_GS>(c, 0);
+    sweep<SW_GS>(c, 1);
     if (fuse_residual) {
-      k_update_res<S, true, true, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
-                                                                                         L.partials);
+      k_sweep_finish<S, true, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
+                                                                                     L.partials);
       residual_final(c);
     } else {
-      k_update_res<S, true, false, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
-                                                                                          L.partials);
+      k_sweep_finish<S, false, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
+                                                                                      L.partials);
     }
+    return 0;
+  }
+
+  static int skew_static(orion_case_t c, int b) {
+    k_skew_static<S><<<148 * 4, kThreads, 0, c->stream>>>(blocks(c), b);
     return 0;
   }
 
@@ -900,6 +974,11 @@ int orion_case_upload(orion_case_t c, int block, int field, const double* host) 
     CUDA_TRY(cudaMemcpy(d, tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice));
   } else {
     CUDA_TRY(cudaMemcpy(d, host, n * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  if (field == ORION_FIELD_METRICS || field == ORION_FIELD_VOL) {
+    rc = dispatch(c, [&] { return Plain::skew_static(c, block); }, [&] { return Mixed::skew_static(c, block); });
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
   }
   return 0;
 }
