@@ -72,6 +72,8 @@ SIGNATURES = {
     "orion_step": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Residual)]),
     "orion_step_async": (C.c_int, [C.c_void_p, C.c_int]),
     "orion_last_residual": (C.c_int, [C.c_void_p, C.POINTER(Residual)]),
+    "orion_residual_block_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                               C.c_void_p, C.POINTER(Residual)]),
 }
 
 _lib = None

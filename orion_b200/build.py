@@ -63,6 +63,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     # device TUs
     units = {
         "orion_gpu.cu": ["--fmad=false"],
+        "noalloc.cu": ["--fmad=false"],
     }
     for name, extra in units.items():
         obj = os.path.join(OBJDIR, name + ".o")
