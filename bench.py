@@ -235,7 +235,7 @@ def main():
         if name == "mixed":
             clocks.start()
         ms = timed_steps(fs, K)
-        results[name] = {"ms": ms, "launches": fs.step_launches(), "fs": fs}
+        results[name] = {"ms": ms, "launches": fs.step_launches(), "fs": fs, "sweeps": fs.sweep_schedule()}
         states[name] = [fs.download(b, "prim")[:5, 3:-3, 3:-3, 3:-3] for b in range(len(case.blocks))]
         if name == "plain":
             clk = clocks.stop()
@@ -328,6 +328,7 @@ def main():
                                    (fsm.footprint() / 1e9)},
             "plain_fp64": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_ms / K, "dtype": "f64"},
             "mixed_over_plain": plain_ms / mixed_ms,
+            "sweep_schedule": {"mixed": results["mixed"]["sweeps"], "plain": results["plain"]["sweeps"]},
             "mixed_vs_plain_rel_l2": l2,
             "roofline": roofline, "step_roofline": step_roofline,
             "stage_ms": stage_ms,

@@ -124,6 +124,11 @@ int orion_case_sync(orion_case_t c);
 int orion_case_stream(orion_case_t c, void** stream);
 /* Kernel launches one captured step issues (after the first orion_step). */
 int orion_case_step_launches(orion_case_t c, int* n);
+/* How the implicit sweeps are scheduled: out[0] = mode (0 one launch per
+ * hyperplane, 1 persistent cooperative grid, 2 thread-block clusters),
+ * out[1] = CTAs (grid) or clusters, out[2] = CTAs per cluster, out[3] = threads
+ * per CTA, out[4] = hyperplanes of the longest sweep.  Waits for set-up only. */
+int orion_case_sweep_schedule(orion_case_t c, int out[5]);
 /* Device bytes held by the case (the HBM footprint used for admission). */
 int orion_case_footprint(orion_case_t c, size_t* bytes);
 size_t orion_footprint_estimate(int nblocks, const orion_block_desc_t* blocks, int precision);

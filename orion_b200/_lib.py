@@ -8,7 +8,7 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "liborion_gpu.so")
+LIB_PATH = os.environ.get("ORION_GPU_LIB") or os.path.join(HERE, "liborion_gpu.so")
 
 PREC_FP64 = 0
 PREC_MIXED = 1
@@ -53,6 +53,7 @@ SIGNATURES = {
     "orion_case_footprint": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "orion_case_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "orion_case_step_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "orion_case_sweep_schedule": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "orion_footprint_estimate": (C.c_size_t, [C.c_int, C.POINTER(BlockDesc), C.c_int]),
     "orion_case_upload": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "orion_case_download": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),

@@ -53,34 +53,41 @@ def _run(cmd):
     return r.stdout + r.stderr
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not _stale():
+def build(force: bool = False, verbose: bool = False, out: str = None, defines=()) -> str:
+    lib = out or LIB
+    if not force and out is None and not _stale():
         return LIB
     nvcc = _nvcc()
     os.makedirs(OBJDIR, exist_ok=True)
-    common = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC]
+    common = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC,
+              *[f"-D{d}" for d in defines]]
+    objdir = OBJDIR if out is None else out + ".objs"
+    os.makedirs(objdir, exist_ok=True)
     objs = []
     # device TUs
+    strict = ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"]
     units = {
-        "orion_gpu.cu": ["--fmad=false"],
-        "noalloc.cu": ["--fmad=false"],
+        "orion_gpu.cu": strict,
+        "stages_fp64.cu": strict,
+        "stages_mixed.cu": ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
+        "noalloc.cu": strict,
     }
     for name, extra in units.items():
-        obj = os.path.join(OBJDIR, name + ".o")
-        out = _run([nvcc, *ARCH, *common, *extra, "-Xptxas", "-v", "-c", os.path.join(CSRC, name), "-o", obj])
+        obj = os.path.join(objdir, name + ".o")
+        log = _run([nvcc, *ARCH, *common, *extra, "-Xptxas", "-v", "-c", os.path.join(CSRC, name), "-o", obj])
         if verbose:
-            print(out)
+            print(log)
         objs.append(obj)
     # host set-up code: plain C++ without contraction
     for name in ("metrics_host.cpp",):
-        obj = os.path.join(OBJDIR, name + ".o")
+        obj = os.path.join(objdir, name + ".o")
         _run(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-I", INCLUDE, "-c",
               os.path.join(CSRC, name), "-o", obj])
         objs.append(obj)
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     _run([nvcc, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", tmp, "-lcudart"])
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":

@@ -1,0 +1,137 @@
+// Host-side case object and shared runtime helpers of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "device_types.cuh"
+#include "orion_gpu.h"
+#include "topology.hpp"
+
+namespace orion {
+
+extern thread_local std::string g_last_error;
+
+inline int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+int set_error(int code, const std::string& msg);
+
+#define CUDA_TRY(expr)                                                                       \
+  do {                                                                                       \
+    cudaError_t _e = (expr);                                                                 \
+    if (_e != cudaSuccess)                                                                   \
+      return ::orion::fail(ORION_E_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+constexpr int kThreads = 256;
+constexpr int kChunk = 256;         // points per CTA (one per thread) for pointwise kernels
+constexpr int kHistCap = 4096;      // residual history ring
+constexpr size_t kLineSmemBudget = 96 * 1024;
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+struct DeviceLists {
+  Chunk* pad_chunks = nullptr;
+  int n_pad_chunks = 0;
+  Chunk* int_chunks = nullptr;
+  int n_int_chunks = 0;
+  LineTile* tiles[3] = {nullptr, nullptr, nullptr};
+  int n_tiles[3] = {0, 0, 0};
+  int lanes[3] = {1, 1, 1};
+  int lmax[3] = {0, 0, 0};
+  Chunk* sweep_chunks[2] = {nullptr, nullptr};  // forward / backward hyperplane launches
+  std::vector<int> sweep_off[2];                 // host: chunk range of each launch
+  int* sweep_off_dev[2] = {nullptr, nullptr};    // device copies of sweep_off
+  void* sweep_ctl = nullptr;                     // SweepCtl of the persistent sweep kernel
+  int persist_grid = 0;                          // CTAs of the persistent sweep kernel (0: per-plane launches)
+  int sweep_nt = 256;                            // threads per sweep CTA = hyperplane chunk size
+  // cluster sweeps: mesh blocks grouped per thread-block cluster
+  int cl_size = 0;                               // CTAs per cluster (0: not used)
+  int cl_count = 0;                              // clusters (= groups)
+  Chunk* cl_chunks[2] = {nullptr, nullptr};      // forward / backward chunk lists of all groups
+  int* cl_off[2] = {nullptr, nullptr};           // per-group hyperplane offsets, concatenated
+  int* cl_base = nullptr;                        // start of each group's offsets
+  int* cl_nplanes = nullptr;                     // hyperplanes of each group
+  long long spin_limit = 1LL << 21;              // polls before a grid barrier gives up (about a second)
+  int max_planes = 0;
+  long long* halo_src = nullptr;
+  long long* halo_dst = nullptr;
+  int n_halo = 0;
+  RegionDev* regions = nullptr;
+  int* phase_regions = nullptr;
+  std::vector<int> phase_off;  // host: region list offsets per phase
+  std::vector<int> phase_maxpts;
+  int* pk_block = nullptr;
+  long long* pk_idx = nullptr;
+  double* pack = nullptr;
+  int n_pack = 0;
+  int* ap_block = nullptr;
+  long long* ap_idx = nullptr;
+  int* ap_off = nullptr;
+  int* ap_slot = nullptr;
+  int n_ap = 0;
+  ResPartial* partials = nullptr;
+  ResidualOut* hist = nullptr;
+  int* counter = nullptr;
+  unsigned long long* dtmin = nullptr;
+  double* dt_part = nullptr;  // per-CTA minima of dt_phys
+  long long* pad_base = nullptr;
+};
+
+}  // namespace orion
+
+struct orion_case_s {
+  int nblocks = 0;
+  int prec = ORION_PREC_FP64;
+  orion::ParamsDev P{};
+  std::vector<orion::HostBlock> hb;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int device = 0;
+  void* arena = nullptr;
+  size_t arena_bytes = 0;
+  std::vector<void*> allocs;  // other device allocations
+  std::vector<orion::BlockDev<double>> bd64;
+  std::vector<orion::BlockDev<float>> bd32;
+  void* d_blocks = nullptr;
+  orion::DeviceLists L;
+  long long total_interior = 0;
+  cudaGraphExec_t graph = nullptr;
+  long long steps_done = 0;
+  int step_launches = 0;
+};
+
+namespace orion {
+
+// Launchers of one precision (plain FP64 or mixed), compiled in their own
+// translation unit with that precision's floating-point flags.
+struct StageOps {
+  int (*set_attributes)();
+  int (*exchange)(orion_case_t);
+  int (*bc)(orion_case_t);
+  int (*state)(orion_case_t, bool with_dt, bool with_q);
+  int (*timestep)(orion_case_t);
+  int (*viscous)(orion_case_t);
+  int (*average)(orion_case_t);
+  int (*inviscid)(orion_case_t);
+  int (*update)(orion_case_t, bool fuse_residual);
+  int (*residual)(orion_case_t);
+  int (*step)(orion_case_t, bool with_q);
+  int (*init_flow)(orion_case_t, uint64_t seed, double amp);
+  int (*skew_static)(orion_case_t, int block);
+  int (*persistent_grid)(orion_case_t);
+};
+
+// Groups the mesh blocks into `nclusters` clusters (largest first onto the
+// least-loaded cluster) and uploads each group's hyperplane chunk lists.
+int build_cluster_lists(orion_case_t c, int nclusters);
+
+const StageOps& plain_ops();
+const StageOps& mixed_ops();
+
+}  // namespace orion

@@ -35,6 +35,7 @@ struct BlockDev {
   long long ncomp;        // ni * nj * nk
   const int* koff;        // start of run (s, kk) at koff[s * nk + kk]; koff[nplanes * nk] = ncomp
   const int* sk_nat;      // padded natural index of each compact point
+  const int* sk_nb;       // 6 comps: compact index of the face neighbours (lower i,j,k, upper i,j,k), -1 outside
   S* sk_metrics;          // 9 comps (static)
   S* sk_vol;              // static
   S* sk_prim;             // 5 comps
@@ -42,6 +43,11 @@ struct BlockDev {
   S* sk_coed;             // diagonal coefficient
   S* sk_rhs;              // 5 comps: masked RHS
   S* sk_dq;               // 5 comps: the increment being swept
+  // Coefficients of the flux splitting that do not involve the swept increment
+  // (computed once per step, off the sweeps' critical path):
+  S* sk_nrm;              // 9 (static): unit normal nx_n,ny_n,nz_n of the point's xi, eta, zeta metrics
+  S* sk_nbq;              // 6: u, v, w, H, c^2, (gamma-1)/2 v^2 of the point as somebody's neighbour
+  S* sk_pair;             // 30: per face neighbour q (lower i,j,k, upper i,j,k): l1, x1, x2, ct_n, rv/2
 };
 
 // Scalar parameters (orion_params_t after conversion).

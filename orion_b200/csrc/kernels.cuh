@@ -3,6 +3,7 @@
 // (double for the plain form, float for the mixed form), T = compute type of
 // the flux / viscous / sweep arithmetic.
 #pragma once
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -299,28 +300,31 @@ __global__ void k_bc_phase(const BlockDev<S>* __restrict__ blocks, const RegionD
 // ===========================================================================
 template <typename S, bool DO_Q>
 __device__ __forceinline__ void state_point(const BlockDev<S>& B, const ParamsDev& P, long long idx, int i, int j,
-                                            int k, double& c_out, double& mu_out) {
+                                            int k, S& c_out, S& mu_out) {
+  // arithmetic in the storage precision S of c, mu, dt (FP64 on the plain path)
   const long long np = B.npad;
   const bool inI = (i >= NG && i < NG + B.ni), inJ = (j >= NG && j < NG + B.nj), inK = (k >= NG && k < NG + B.nk);
   const int nin = (int)inI + (int)inJ + (int)inK;
   double* prim = B.prim;
-  double T = prim[5 * np + idx];
-  double cval = (double)B.c[idx];
+  const S gamma = (S)P.gamma, moo = (S)P.moo, visc = (S)P.visc;
+  S T = (S)prim[5 * np + idx];
+  S cval = B.c[idx];
   if (nin >= 2) {
     // interior (nin == 3) or ghost face slab (nin == 2), update_thermodynamics_block
-    double rho = prim[idx];
-    const double p = prim[4 * np + idx];
-    if (nin == 2) rho = fabs(rho);
-    const double a2 = P.gamma * p / rho;
-    cval = sqrt(fabs(a2));
-    B.c[idx] = (S)cval;
+    S rho = (S)__ldg(prim + idx);
+    const S p = (S)__ldg(prim + 4 * np + idx);
+    if (nin == 2) rho = tabs(rho);
+    const S a2 = gamma * p / rho;
+    cval = tsqrt(tabs(a2));
+    B.c[idx] = cval;
     if (P.nvis == 1) {
-      T = (P.moo * P.moo) * a2;
-      prim[5 * np + idx] = T;
+      T = (moo * moo) * a2;
+      prim[5 * np + idx] = (double)T;
     }
     if (DO_Q) {
-      // update_conservative_block (StateUpdater.cpp:94-149)
-      const double r0 = prim[idx], u = prim[np + idx], v = prim[2 * np + idx], w = prim[3 * np + idx];
+      // update_conservative_block (StateUpdater.cpp:94-149), FP64
+      const double r0 = __ldg(prim + idx), u = __ldg(prim + np + idx), v = __ldg(prim + 2 * np + idx),
+                   w = __ldg(prim + 3 * np + idx), pd = __ldg(prim + 4 * np + idx);
       const bool use_abs = (nin == 2);
       const double rc = (use_abs || r0 < 0.0) ? fabs(r0) : r0;
       const double gm1_inv = 1.0 / (P.gamma - 1.0);
@@ -329,16 +333,16 @@ __device__ __forceinline__ void state_point(const BlockDev<S>& B, const ParamsDe
       B.q[2 * np + idx] = rc * v;
       B.q[3 * np + idx] = rc * w;
       const double ke = 0.5 * rc * (u * u + v * v + w * w);
-      B.q[4 * np + idx] = p * gm1_inv + ke;
+      B.q[4 * np + idx] = pd * gm1_inv + ke;
     }
   }
-  double muv = (double)B.mu[idx];
+  S muv = B.mu[idx];
   if (P.nvis == 1) {
     // update_viscosity_block (StateUpdater.cpp:75-92): whole padded array
-    double tm = T;
-    if (tm < 1e-6) tm = 1e-6;
-    muv = tm * sqrt(tm) * (1.0 + P.visc) / (tm + P.visc);
-    B.mu[idx] = (S)muv;
+    S tm = T;
+    if (tm < S(1e-6)) tm = S(1e-6);
+    muv = tm * tsqrt(tm) * (S(1) + visc) / (tm + visc);
+    B.mu[idx] = muv;
   }
   for (int m = 0; m < 5; ++m) B.dq[m * np + idx] = (S)0;
   c_out = cval;
@@ -346,86 +350,116 @@ __device__ __forceinline__ void state_point(const BlockDev<S>& B, const ParamsDe
 }
 
 template <typename S>
-__device__ __forceinline__ double timestep_point(const BlockDev<S>& B, const ParamsDev& P, long long idx, double c,
-                                                 double mu) {
+__device__ __forceinline__ S timestep_point(const BlockDev<S>& B, const ParamsDev& P, long long idx, S c, S mu) {
   // calculate_spectrum + calculate_local_dt_cell (TimeIntegrator.cpp:20-125)
   const long long np = B.npad;
-  const double u = B.prim[np + idx], v = B.prim[2 * np + idx], w = B.prim[3 * np + idx];
-  const double rho = B.prim[idx];
-  const double vol = B.vol[idx];
-  double sum_spec = 0.0;
+  const S u = (S)__ldg(B.prim + np + idx), v = (S)__ldg(B.prim + 2 * np + idx), w = (S)__ldg(B.prim + 3 * np + idx);
+  const S rho = (S)__ldg(B.prim + idx);
+  const S vol = (S)__ldg(B.vol + idx);
+  const S reynolds = (S)P.reynolds, csrv = (S)P.csrv;
+  S sum_spec = S(0);
   for (int d = 0; d < 3; ++d) {
-    const double mx = B.metrics[(3 * d + 0) * np + idx];
-    const double my = B.metrics[(3 * d + 1) * np + idx];
-    const double mz = B.metrics[(3 * d + 2) * np + idx];
-    const double U_contra = fabs(u * mx + v * my + w * mz);
-    const double grad_len = sqrt(mx * mx + my * my + mz * mz);
-    const double spec = U_contra + c * grad_len;
-    double specv = 0.0;
+    const S mx = (S)__ldg(B.metrics + (3 * d + 0) * np + idx);
+    const S my = (S)__ldg(B.metrics + (3 * d + 1) * np + idx);
+    const S mz = (S)__ldg(B.metrics + (3 * d + 2) * np + idx);
+    const S U_contra = tabs(u * mx + v * my + w * mz);
+    const S grad_len = tsqrt(mx * mx + my * my + mz * mz);
+    const S spec = U_contra + c * grad_len;
+    S specv = S(0);
     if (P.nvis == 1) {
-      const double grad_sq = mx * mx + my * my + mz * mz;
-      const double denom = P.reynolds * rho * vol + 1.0e-30;
-      specv = (2.0 * mu / denom) * grad_sq * P.csrv;
+      const S grad_sq = mx * mx + my * my + mz * mz;
+      const S denom = reynolds * rho * vol + S(1.0e-30);
+      specv = (S(2) * mu / denom) * grad_sq * csrv;
     }
     sum_spec += spec + specv;
   }
-  const double dt_phys = P.cfl / (sum_spec + 1.0e-30);
+  const S dt_phys = (S)P.cfl / (sum_spec + S(1.0e-30));
   return dt_phys / vol;
 }
 
-__device__ __forceinline__ void atomic_min_pos_double(unsigned long long* addr, double v) {
-  // positive doubles order like their bit patterns
-  if (v >= 0.0) atomicMin(addr, (unsigned long long)__double_as_longlong(v));
+// CTA-wide minimum written to part[blockIdx.x] (no same-address atomics: a
+// few thousand of those serialize for milliseconds).
+__device__ __forceinline__ void block_min_to(double v, double* part) {
+  for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, off));
+  __shared__ double s_min[32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) s_min[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    v = (l < nw) ? s_min[l] : 1000.0;
+    for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, off));
+    if (l == 0) part[blockIdx.x] = v;
+  }
+}
+
+// phydtime = min(1000, min over the partials) (TimeIntegrator.cpp:151-176), stored as bits.
+static __global__ void __launch_bounds__(1024) k_dtmin_final(const double* __restrict__ part, int n,
+                                                             unsigned long long* __restrict__ dtmin_bits) {
+  double v = 1000.0;
+  for (int t = threadIdx.x; t < n; t += 1024) v = fmin(v, part[t]);
+  for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, off));
+  __shared__ double s_min[32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) s_min[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = s_min[l];
+    for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, off));
+    if (l == 0) *dtmin_bits = (unsigned long long)__double_as_longlong(v);
+  }
 }
 
 template <typename S, bool DO_Q, bool DO_DT>
 __global__ void k_state(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P,
-                        unsigned long long* __restrict__ dtmin_bits) {
+                        double* __restrict__ dt_part) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
   double local_min = 1000.0;
+#pragma unroll 4
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
     const long long idx = ch.start + t;
-    const int i = (int)(idx % B.nx);
-    const int j = (int)((idx / B.nx) % B.ny);
-    const int k = (int)(idx / ((long long)B.nx * B.ny));
-    double c, mu;
+    const int i32 = (int)idx;  // padded index < 2^31
+    const int i = i32 % B.nx;
+    const int r = i32 / B.nx;
+    const int j = r % B.ny;
+    const int k = r / B.ny;
+    S c, mu;
     state_point<S, DO_Q>(B, P, idx, i, j, k, c, mu);
     if (DO_DT) {
       const bool interior = (i >= NG && i < NG + B.ni && j >= NG && j < NG + B.nj && k >= NG && k < NG + B.nk);
       if (interior) {
-        const double dtv = timestep_point(B, P, idx, c, mu);
-        B.dt[idx] = (S)dtv;
-        const double dt_phys = (double)(S)dtv * B.vol[idx];
+        const S dtv = timestep_point(B, P, idx, c, mu);
+        B.dt[idx] = dtv;
+        const double dt_phys = (double)dtv * B.vol[idx];
         if (dt_phys < local_min) local_min = dt_phys;
       }
     }
   }
-  if (DO_DT) atomic_min_pos_double(dtmin_bits, local_min);
+  if (DO_DT) block_min_to(local_min, dt_part);
 }
 
 // time step alone (per-stage entry point): interior points of interior chunks
 template <typename S>
 __global__ void k_timestep(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P,
-                           unsigned long long* __restrict__ dtmin_bits) {
+                           double* __restrict__ dt_part) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
   double local_min = 1000.0;
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
     const long long n = ch.start + t;  // interior index
-    const int ii = (int)(n % B.ni), jj = (int)((n / B.ni) % B.nj), kk = (int)(n / ((long long)B.ni * B.nj));
+    const int n32 = (int)n, r32 = n32 / B.ni;
+    const int ii = n32 - r32 * B.ni, jj = r32 % B.nj, kk = r32 / B.nj;
     const long long idx = lin(B, NG + ii, NG + jj, NG + kk);
-    const double dtv = timestep_point(B, P, idx, (double)B.c[idx], (double)B.mu[idx]);
-    B.dt[idx] = (S)dtv;
-    const double dt_phys = (double)(S)dtv * B.vol[idx];
+    const S dtv = timestep_point(B, P, idx, B.c[idx], B.mu[idx]);
+    B.dt[idx] = dtv;
+    const double dt_phys = (double)dtv * B.vol[idx];
     if (dt_phys < local_min) local_min = dt_phys;
   }
-  atomic_min_pos_double(dtmin_bits, local_min);
+  block_min_to(local_min, dt_part);
 }
 
-static __global__ void k_step_begin(unsigned long long* dtmin_bits) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) *dtmin_bits = (unsigned long long)__double_as_longlong(1000.0);
-}
 
 // ===========================================================================
 // Node derivatives of (u,v,w,T) along xi, eta, zeta at interior points
@@ -464,7 +498,8 @@ __global__ void k_node_derivs(const BlockDev<S>* __restrict__ blocks, const Chun
   const long long np = B.npad;
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
     const long long n = ch.start + t;
-    const int ii = (int)(n % B.ni), jj = (int)((n / B.ni) % B.nj), kk = (int)(n / ((long long)B.ni * B.nj));
+    const int n32 = (int)n, r32 = n32 / B.ni;
+    const int ii = n32 - r32 * B.ni, jj = r32 % B.nj, kk = r32 / B.nj;
     const long long idx = lin(B, NG + ii, NG + jj, NG + kk);
     const int tt[3] = {ii, jj, kk};
     for (int d = 0; d < 3; ++d) {
@@ -591,8 +626,26 @@ __device__ __forceinline__ void tile_item(int it, int nlanes, int nfaces, int& l
   }
 }
 
+// CTAs per SM the line kernels are compiled for (register cap 65536/(256*n)),
+// per compute precision: FP32 runs best at four, FP64 at three and two.
+#ifndef ORION_VISC_MINB_F32
+#define ORION_VISC_MINB_F32 4
+#endif
+#ifndef ORION_INV_MINB_F32
+#define ORION_INV_MINB_F32 4
+#endif
+#ifndef ORION_VISC_MINB_F64
+#define ORION_VISC_MINB_F64 3
+#endif
+#ifndef ORION_INV_MINB_F64
+#define ORION_INV_MINB_F64 2
+#endif
+template <typename T> struct LineMinBlocks;
+template <> struct LineMinBlocks<float> { static constexpr int visc = ORION_VISC_MINB_F32, inv = ORION_INV_MINB_F32; };
+template <> struct LineMinBlocks<double> { static constexpr int visc = ORION_VISC_MINB_F64, inv = ORION_INV_MINB_F64; };
+
 template <int D, typename S, typename T>
-__global__ void k_viscous(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles, ParamsDev P) {
+__global__ void __launch_bounds__(256, LineMinBlocks<T>::visc) k_viscous(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles, ParamsDev P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* fsh = reinterpret_cast<T*>(smem_raw);
   const LineTile tl = tiles[blockIdx.x];
@@ -730,60 +783,75 @@ __device__ __forceinline__ void fallback_roe(const InvLine<S, T>& ln, int f, T q
 
 // Left-end re-calculation rounds (InviscidFluxComputer.cpp:377-448): the value
 // of fc[t] for t = 0, 1, 2 when the ghost-3 density flag is set.
+// Boundary re-calculation rounds of a flagged line end
+// (InviscidFluxComputer.cpp:377-521).  Each output point needs one round of
+// 4-5 Roe fluxes; every flux is folded into the output as soon as it is
+// computed, in the order and with the coefficients of the reference's formula,
+// so no per-face array is kept.
 template <int D, typename S, typename T>
-__device__ void cascade_left(const BlockDev<S>& B, const InvLine<S, T>& ln, int t, T gamma, T fc[5]) {
-  T F[6][5];
-  auto flux_eq = [&](int f, const T s[5]) {
-    T ql[5], qr[5];
-    for (int m = 0; m < 5; ++m) { ql[m] = s[m]; qr[m] = s[m]; }
-    T kx, ky, kz;
-    face_metric<D, S, T>(B, ln.o, ln.st, f, ln.L, kx, ky, kz);
-    fallback_roe<S, T>(ln, f, ql, qr, kx, ky, kz, gamma, F[f]);
-  };
-  auto flux_lr = [&](int f, const T l[5], const T r[5]) {
-    T ql[5], qr[5];
+struct Cascade {
+  const BlockDev<S>& B;
+  const InvLine<S, T>& ln;
+  T gamma;
+  T acc[5];
+  __device__ __forceinline__ void flux(int f, const T l[5], const T r[5], T coef, bool first) {
+    T ql[5], qr[5], out[5];
     for (int m = 0; m < 5; ++m) { ql[m] = l[m]; qr[m] = r[m]; }
     T kx, ky, kz;
     face_metric<D, S, T>(B, ln.o, ln.st, f, ln.L, kx, ky, kz);
-    fallback_roe<S, T>(ln, f, ql, qr, kx, ky, kz, gamma, F[f]);
-  };
+    fallback_roe<S, T>(ln, f, ql, qr, kx, ky, kz, gamma, out);
+    // acc = coef*F (first term) or acc + coef*F; a coefficient of +1 or -1 is an
+    // exact add or subtract of F as in the reference's expression
+    for (int m = 0; m < 5; ++m) {
+      if (first) acc[m] = coef * out[m];
+      else if (coef == T(1)) acc[m] = acc[m] + out[m];
+      else if (coef == T(-1)) acc[m] = acc[m] - out[m];
+      else acc[m] = acc[m] + coef * out[m];
+    }
+  }
+};
+
+template <int D, typename S, typename T>
+__device__ void cascade_left(const BlockDev<S>& B, const InvLine<S, T>& ln, int t, T gamma, T fc[5]) {
+  Cascade<D, S, T> cs{B, ln, gamma, {}};
   T Q3[5], Q4[5], Q5[5], Q6[5];
   for (int m = 0; m < 5; ++m) { Q3[m] = ln.q(3, m); Q4[m] = ln.q(4, m); Q5[m] = ln.q(5, m); Q6[m] = ln.q(6, m); }
   T s[5], s2[5];
   if (t == 0) {
+    // fc[0] = (-23 F0 + 21 F1 + 3 F2 - F3) / 24 over round-1 states
     for (int m = 0; m < 5; ++m) s[m] = (T(3.) * Q3[m] - T(1.) * Q4[m]) / T(2.0);
-    flux_eq(0, s);
+    cs.flux(0, s, s, T(-23.), true);
     for (int m = 0; m < 5; ++m) s[m] = (T(19.) * Q3[m] + T(25.) * Q4[m] - T(2.) * Q5[m]) / T(42.0);
-    flux_eq(1, s);
+    cs.flux(1, s, s, T(21.), false);
     for (int m = 0; m < 5; ++m) s[m] = (T(4.) * Q3[m] + T(3.) * Q4[m] + T(9.) * Q5[m] + T(2.) * Q6[m]) / T(18.0);
-    flux_eq(2, s);
+    cs.flux(2, s, s, T(3.), false);
     for (int m = 0; m < 5; ++m) s[m] = (T(-2.) * Q3[m] + T(3.) * Q4[m] + T(3.) * Q5[m] + T(2.) * Q6[m]) / T(6.0);
-    flux_eq(3, s);
-    for (int m = 0; m < 5; ++m) fc[m] = (T(-23.) * F[0][m] + T(21.) * F[1][m] + T(3.) * F[2][m] - F[3][m]) / T(24.0);
+    cs.flux(3, s, s, T(-1), false);
   } else if (t == 1) {
+    // fc[1] = (-22 F1 + 17 F2 + 9 F3 - 5 F4 + F5) / 24 over round-2 states
     for (int m = 0; m < 5; ++m) s[m] = (T(3.) * Q3[m] + T(6.) * Q4[m] - Q5[m]) / T(8.0);
-    flux_eq(1, s);
+    cs.flux(1, s, s, T(-22.), true);
     for (int m = 0; m < 5; ++m) {
       s[m] = (T(-30.) * Q3[m] + T(145.) * Q4[m] + T(29.) * Q5[m] - T(8.) * Q6[m]) / T(136.0);
       s2[m] = (T(2.) * Q3[m] + T(49.) * Q4[m] + T(125.) * Q5[m] - T(40.) * Q6[m]) / T(136.0);
     }
-    flux_lr(2, s, s2);
+    cs.flux(2, s, s2, T(17.), false);
     for (int m = 0; m < 5; ++m) s[m] = (-Q4[m] + T(6.) * Q5[m] + T(3.) * Q6[m]) / T(8.0);
-    flux_eq(3, s);
+    cs.flux(3, s, s, T(9.), false);
     for (int m = 0; m < 5; ++m) s[m] = (Q4[m] + T(2.) * Q5[m] + T(5.) * Q6[m]) / T(8.0);
-    flux_eq(4, s);
+    cs.flux(4, s, s, T(-5.), false);
     for (int m = 0; m < 5; ++m) s[m] = (Q4[m] + Q5[m] + T(6.) * Q6[m]) / T(8.0);
-    flux_eq(5, s);
-    for (int m = 0; m < 5; ++m)
-      fc[m] = (T(-22.) * F[1][m] + T(17.) * F[2][m] + T(9.) * F[3][m] - T(5.) * F[4][m] + F[5][m]) / T(24.0);
+    cs.flux(5, s, s, T(1), false);
   } else {
-    // face 1: left from round 2, right restored (fixed 5,15,-5,1 stencil)
+    // fc[2] = (F1 - 27 F2 + 27 F3 - F4) / 24 over round-3 states; face 1 keeps the
+    // round-2 left state and the restored fixed right state, faces 2..4 the
+    // restored WCNS right states
     for (int m = 0; m < 5; ++m) {
       s[m] = (T(3.) * Q3[m] + T(6.) * Q4[m] - Q5[m]) / T(8.0);
       s2[m] = (T(5.) * Q3[m] + T(15.) * Q4[m] - T(5.) * Q5[m] + Q6[m]) / T(16.);
     }
-    flux_lr(1, s, s2);
-    // faces 2..4: right restored = WCNS right state of the main pass
+    cs.flux(1, s, s2, T(1), true);
+    const T coef[3] = {T(-27.), T(27.), T(-1)};
     for (int f = 2; f <= 4; ++f) {
       for (int m = 0; m < 5; ++m) {
         if (f == 2) s[m] = (T(-29.) * Q3[m] + T(170.) * Q4[m] + T(63.) * Q5[m] + T(12.) * Q6[m]) / T(216.0);
@@ -791,64 +859,54 @@ __device__ void cascade_left(const BlockDev<S>& B, const InvLine<S, T>& ln, int 
         else s[m] = (Q4[m] + T(2.) * Q5[m] + T(5.) * Q6[m]) / T(8.0);
         s2[m] = wcns_right<T>(ln.q(f + 1, m), ln.q(f + 2, m), ln.q(f + 3, m), ln.q(f + 4, m), ln.q(f + 5, m));
       }
-      flux_lr(f, s, s2);
+      cs.flux(f, s, s2, coef[f - 2], false);
     }
-    for (int m = 0; m < 5; ++m) fc[m] = (F[1][m] - T(27.) * F[2][m] + T(27.) * F[3][m] - F[4][m]) / T(24.0);
   }
+  for (int m = 0; m < 5; ++m) fc[m] = cs.acc[m] / T(24.0);
 }
 
-// Right-end re-calculation rounds (InviscidFluxComputer.cpp:450-521): fc[t] for
-// t = L-1, L-2, L-3.  Faces are stored at F[N - f'] with f' the face index.
 template <int D, typename S, typename T>
 __device__ void cascade_right(const BlockDev<S>& B, const InvLine<S, T>& ln, int t, T gamma, T fc[5]) {
   const int N = ln.L;
-  T F[6][5];  // F[a] = flux at face N - a
-  auto flux_at = [&](int f, const T l[5], const T r[5]) {
-    T ql[5], qr[5];
-    for (int m = 0; m < 5; ++m) { ql[m] = l[m]; qr[m] = r[m]; }
-    T kx, ky, kz;
-    face_metric<D, S, T>(B, ln.o, ln.st, f, ln.L, kx, ky, kz);
-    fallback_roe<S, T>(ln, f, ql, qr, kx, ky, kz, gamma, F[N - f]);
-  };
+  Cascade<D, S, T> cs{B, ln, gamma, {}};
   T Qn[5], Qn1[5], Qn2[5], Qn3[5];
   for (int m = 0; m < 5; ++m) {
     Qn[m] = ln.q(N + 2, m); Qn1[m] = ln.q(N + 1, m); Qn2[m] = ln.q(N, m); Qn3[m] = ln.q(N - 1, m);
   }
   T s[5], s2[5];
   if (t == N - 1) {
+    // fc[N-1] = -(-23 F[N] + 21 F[N-1] + 3 F[N-2] - F[N-3]) / 24
     for (int m = 0; m < 5; ++m) s[m] = (T(3.) * Qn[m] - T(1.) * Qn1[m]) / T(2.0);
-    flux_at(N, s, s);
+    cs.flux(N, s, s, T(-23.), true);
     for (int m = 0; m < 5; ++m) s[m] = (T(19.) * Qn[m] + T(25.) * Qn1[m] - T(2.) * Qn2[m]) / T(42.0);
-    flux_at(N - 1, s, s);
+    cs.flux(N - 1, s, s, T(21.), false);
     for (int m = 0; m < 5; ++m) s[m] = (T(4.) * Qn[m] + T(3.) * Qn1[m] + T(9.) * Qn2[m] + T(2.) * Qn3[m]) / T(18.0);
-    flux_at(N - 2, s, s);
+    cs.flux(N - 2, s, s, T(3.), false);
     for (int m = 0; m < 5; ++m) s[m] = (T(-2.) * Qn[m] + T(3.) * Qn1[m] + T(3.) * Qn2[m] + T(2.) * Qn3[m]) / T(6.0);
-    flux_at(N - 3, s, s);
-    for (int m = 0; m < 5; ++m)
-      fc[m] = -(T(-23.) * F[0][m] + T(21.) * F[1][m] + T(3.) * F[2][m] - F[3][m]) / T(24.0);
+    cs.flux(N - 3, s, s, T(-1), false);
   } else if (t == N - 2) {
+    // fc[N-2] = -(-22 F[N-1] + 17 F[N-2] + 9 F[N-3] - 5 F[N-4] + F[N-5]) / 24
     for (int m = 0; m < 5; ++m) s[m] = (T(3.) * Qn[m] + T(6.) * Qn1[m] - Qn2[m]) / T(8.0);
-    flux_at(N - 1, s, s);
+    cs.flux(N - 1, s, s, T(-22.), true);
     for (int m = 0; m < 5; ++m) {
       s2[m] = (T(-30.) * Qn[m] + T(145.) * Qn1[m] + T(29.) * Qn2[m] - T(8.) * Qn3[m]) / T(136.0);  // right
       s[m] = (T(2.) * Qn[m] + T(49.) * Qn1[m] + T(125.) * Qn2[m] - T(40.) * Qn3[m]) / T(136.0);    // left
     }
-    flux_at(N - 2, s, s2);
+    cs.flux(N - 2, s, s2, T(17.), false);
     for (int m = 0; m < 5; ++m) s[m] = (-Qn1[m] + T(6.) * Qn2[m] + T(3.) * Qn3[m]) / T(8.0);
-    flux_at(N - 3, s, s);
+    cs.flux(N - 3, s, s, T(9.), false);
     for (int m = 0; m < 5; ++m) s[m] = (Qn1[m] + T(2.) * Qn2[m] + T(5.) * Qn3[m]) / T(8.0);
-    flux_at(N - 4, s, s);
+    cs.flux(N - 4, s, s, T(-5.), false);
     for (int m = 0; m < 5; ++m) s[m] = (Qn1[m] + Qn2[m] + T(6.) * Qn3[m]) / T(8.0);
-    flux_at(N - 5, s, s);
-    for (int m = 0; m < 5; ++m)
-      fc[m] = -(T(-22.) * F[1][m] + T(17.) * F[2][m] + T(9.) * F[3][m] - T(5.) * F[4][m] + F[5][m]) / T(24.0);
+    cs.flux(N - 5, s, s, T(1), false);
   } else {
-    // face N-1: right from round 2, left restored (fixed 5,15,-5,1 stencil)
+    // fc[N-3] = -(F[N-1] - 27 F[N-2] + 27 F[N-3] - F[N-4]) / 24
     for (int m = 0; m < 5; ++m) {
       s2[m] = (T(3.) * Qn[m] + T(6.) * Qn1[m] - Qn2[m]) / T(8.0);
       s[m] = (T(5.) * Qn[m] + T(15.) * Qn1[m] - T(5.) * Qn2[m] + Qn3[m]) / T(16.);
     }
-    flux_at(N - 1, s, s2);
+    cs.flux(N - 1, s, s2, T(1), true);
+    const T coef[3] = {T(-27.), T(27.), T(-1)};
     for (int f = N - 2; f >= N - 4; --f) {
       for (int m = 0; m < 5; ++m) {
         if (f == N - 2) s2[m] = (T(-29.) * Qn[m] + T(170.) * Qn1[m] + T(63.) * Qn2[m] + T(12.) * Qn3[m]) / T(216.0);
@@ -856,14 +914,14 @@ __device__ void cascade_right(const BlockDev<S>& B, const InvLine<S, T>& ln, int
         else s2[m] = (Qn1[m] + T(2.) * Qn2[m] + T(5.) * Qn3[m]) / T(8.0);
         s[m] = wcns_left<T>(ln.q(f, m), ln.q(f + 1, m), ln.q(f + 2, m), ln.q(f + 3, m), ln.q(f + 4, m));
       }
-      flux_at(f, s, s2);
+      cs.flux(f, s, s2, coef[N - 2 - f], false);
     }
-    for (int m = 0; m < 5; ++m) fc[m] = -(F[1][m] - T(27.) * F[2][m] + T(27.) * F[3][m] - F[4][m]) / T(24.0);
   }
+  for (int m = 0; m < 5; ++m) fc[m] = -cs.acc[m] / T(24.0);
 }
 
 template <int D, typename S, typename T>
-__global__ void k_inviscid(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles, ParamsDev P) {
+__global__ void __launch_bounds__(256, LineMinBlocks<T>::inv) k_inviscid(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles, ParamsDev P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* fsh = reinterpret_cast<T*>(smem_raw);
   const LineTile tl = tiles[blockIdx.x];
@@ -888,25 +946,37 @@ __global__ void k_inviscid(const BlockDev<S>* __restrict__ blocks, const LineTil
     for (int m = 0; m < 5; ++m) dst[m] = fo[m];
   }
   __syncthreads();
+  // regular points: flux difference of the face fluxes
   const int npts = tl.count * L;
   for (int it = threadIdx.x; it < npts; it += blockDim.x) {
     int lane, t;
     tile_item<D>(it, tl.count, L, lane, t);
     const long long o = line_origin(B, D, tl.first + lane);
-    const long long idx = o + (long long)(t + NG) * st;
     const bool fl = B.prim[o] < 1.0e-20;
     const bool fr = B.prim[o + (long long)(L + 5) * st] < 1.0e-20;
-    T fc[5];
-    if (fl && t <= 2) {
-      InvLine<S, T> ln{B.prim, o, st, B.npad, L};
-      cascade_left<D, S, T>(B, ln, t, gamma, fc);
-    } else if (fr && t >= L - 3) {
-      InvLine<S, T> ln{B.prim, o, st, B.npad, L};
-      cascade_right<D, S, T>(B, ln, t, gamma, fc);
-    } else {
-      const T* fb = fsh + (size_t)lane * nf * 5;
-      for (int m = 0; m < 5; ++m) fc[m] = flux_diff<T>(fb + m, 5, t, L);
+    if ((fl && t <= 2) || (fr && t >= L - 3)) continue;  // re-calculated below
+    const long long idx = o + (long long)(t + NG) * st;
+    const T* fb = fsh + (size_t)lane * nf * 5;
+    for (int m = 0; m < 5; ++m) {
+      S* q = B.dq + m * B.npad + idx;
+      *q = (S)((T)*q + flux_diff<T>(fb + m, 5, t, L));
     }
+  }
+  // boundary re-calculation of flagged line ends, six outputs per line handled
+  // by consecutive threads so the rounds do not stall the regular warps
+  const int nbnd = tl.count * 6;
+  for (int it = threadIdx.x; it < nbnd; it += blockDim.x) {
+    const int lane = it / 6, slot = it - lane * 6;
+    const long long o = line_origin(B, D, tl.first + lane);
+    const bool left = slot < 3;
+    const bool flag = left ? (B.prim[o] < 1.0e-20) : (B.prim[o + (long long)(L + 5) * st] < 1.0e-20);
+    if (!flag) continue;
+    const int t = left ? slot : L - 6 + slot;
+    InvLine<S, T> ln{B.prim, o, st, B.npad, L};
+    T fc[5];
+    if (left) cascade_left<D, S, T>(B, ln, t, gamma, fc);
+    else cascade_right<D, S, T>(B, ln, t, gamma, fc);
+    const long long idx = o + (long long)(t + NG) * st;
     for (int m = 0; m < 5; ++m) {
       S* q = B.dq + m * B.npad + idx;
       *q = (S)((T)*q + fc[m]);
@@ -974,7 +1044,10 @@ __device__ __forceinline__ void decode_nat(const BlockDev<S>& B, int nat, int& i
   kk = r / B.ny - NG;
 }
 
-// Static skewed operands (metrics, vol): refreshed whenever they are uploaded.
+__device__ __forceinline__ double sqrt_s(double x) { return sqrt(x); }
+__device__ __forceinline__ float sqrt_s(float x) { return sqrtf(x); }
+
+// Static skewed operands (metrics, vol, unit normals): refreshed whenever they are uploaded.
 template <typename S>
 __global__ void k_skew_static(const BlockDev<S>* __restrict__ blocks, int b) {
   const BlockDev<S> B = blocks[b];
@@ -982,6 +1055,17 @@ __global__ void k_skew_static(const BlockDev<S>* __restrict__ blocks, int b) {
     const int nat = B.sk_nat[c];
     for (int m = 0; m < 9; ++m) B.sk_metrics[m * B.ncomp + c] = (S)B.metrics[m * B.npad + nat];
     B.sk_vol[c] = (S)B.vol[nat];
+    // unit normals of compute_flux_splitting (StateUpdater.cpp:231-249), per direction
+    for (int d = 0; d < 3; ++d) {
+      const S nx = B.sk_metrics[(3 * d) * B.ncomp + c], ny = B.sk_metrics[(3 * d + 1) * B.ncomp + c],
+              nz = B.sk_metrics[(3 * d + 2) * B.ncomp + c];
+      S grad_mag = sqrt_s(nx * nx + ny * ny + nz * nz);
+      if (grad_mag < S(1.0e-30)) grad_mag = S(1.0e-30);
+      const S inv_mag = S(1) / grad_mag;
+      B.sk_nrm[(3 * d) * B.ncomp + c] = nx * inv_mag;
+      B.sk_nrm[(3 * d + 1) * B.ncomp + c] = ny * inv_mag;
+      B.sk_nrm[(3 * d + 2) * B.ncomp + c] = nz * inv_mag;
+    }
   }
 }
 
@@ -1025,6 +1109,83 @@ __global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk
     const T rad_sum = ra + rb + rc + rva + rvb + rvc;
     const T term = (T(1) / (T)B.dt[nat]) + rad_sum;
     B.sk_coed[c] = (S)(T(1) / term);
+    // the point's quantities as a neighbour in compute_flux_splitting (StateUpdater.cpp:217-253)
+    {
+      T rm = rho, pm = p;
+      const T v2 = u * u + v * v + w * w;
+      if (rm < T(1e-30)) rm = T(1e-30);
+      if (pm < T(1e-30)) pm = T(1e-30);
+      const T c2 = gamma * pm / rm;
+      const T H = (gamma / (gamma - T(1))) * (pm / rm) + T(0.5) * v2;
+      const T af = T(0.5) * (gamma - T(1)) * v2;
+      B.sk_nbq[c] = (S)u;
+      B.sk_nbq[nc + c] = (S)v;
+      B.sk_nbq[2 * nc + c] = (S)w;
+      B.sk_nbq[3 * nc + c] = (S)H;
+      B.sk_nbq[4 * nc + c] = (S)c2;
+      B.sk_nbq[5 * nc + c] = (S)af;
+    }
+  }
+}
+
+// Per face neighbour q of every point: the increment-independent coefficients of
+// add_nb / add_nb_contrib (StateUpdater.cpp:326-343, 401-421): spectral radius of
+// the neighbour with the point's metric, split eigenvalues l1 (and l4, l5 through
+// x1, x2), ct_n, and half the viscous radius.  q = 0..2 lower i,j,k (sign +1),
+// q = 3..5 upper (sign -1).
+template <typename S, typename T>
+__global__ void k_sweep_pairs(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P) {
+  const Chunk ch = chunks[blockIdx.x];
+  const BlockDev<S> B = blocks[ch.block];
+  const long long nc = B.ncomp;
+  const T gamma = T(P.gamma);
+  for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+    const long long c = ch.start + t;
+    int nb[6];
+    for (int q = 0; q < 6; ++q) nb[q] = B.sk_nb[q * nc + c];
+    for (int q = 0; q < 6; ++q) {
+      if (nb[q] < 0) continue;
+      const long long n = nb[q];
+      const int d = q % 3;
+      const T nx = (T)B.sk_metrics[(3 * d) * nc + c], ny = (T)B.sk_metrics[(3 * d + 1) * nc + c],
+              nz = (T)B.sk_metrics[(3 * d + 2) * nc + c];
+      const T rho = (T)B.sk_prim[n], um = (T)B.sk_prim[nc + n], vm = (T)B.sk_prim[2 * nc + n],
+              wm = (T)B.sk_prim[3 * nc + n], p = (T)B.sk_prim[4 * nc + n];
+      const T r = spectral_radius<T>(rho, um, vm, wm, p, gamma, nx, ny, nz);
+      const T sign = q < 3 ? T(1) : T(-1);
+      // compute_flux_splitting up to the increment-dependent part
+      T rm = rho, pm = p;
+      if (rm < T(1e-30)) rm = T(1e-30);
+      if (pm < T(1e-30)) pm = T(1e-30);
+      const T c2 = gamma * pm / rm;
+      const T cm = tsqrt(c2);
+      const T ct = nx * um + ny * vm + nz * wm + T(0);
+      T grad_mag = tsqrt(nx * nx + ny * ny + nz * nz);
+      if (grad_mag < T(1.0e-30)) grad_mag = T(1.0e-30);
+      T l1 = ct;
+      T l4 = ct + cm * grad_mag;
+      T l5 = ct - cm * grad_mag;
+      l1 = T(0.5) * (l1 + sign * r);
+      l4 = T(0.5) * (l4 + sign * r);
+      l5 = T(0.5) * (l5 + sign * r);
+      const T x1 = (T(2) * l1 - l4 - l5) / (T(2) * c2);
+      const T x2 = (l4 - l5) / (T(2) * cm);
+      const T inv_mag = T(1) / grad_mag;
+      const T ct_n = (ct - T(0)) * inv_mag;
+      T rvh = T(0);
+      if (P.nvis == 1) {
+        T vol_nb = (T)B.sk_vol[n];
+        if (vol_nb < T(1e-30)) vol_nb = T(1e-30);
+        const T rv = visc_spectral_radius<T>(rho, (T)B.sk_mu[n], vol_nb, T(P.reynolds), nx, ny, nz);
+        rvh = T(0.5) * rv;
+      }
+      S* out = B.sk_pair + (long long)(5 * q) * nc + c;
+      out[0] = (S)l1;
+      out[nc] = (S)x1;
+      out[2 * nc] = (S)x2;
+      out[3 * nc] = (S)ct_n;
+      out[4 * nc] = (S)rvh;
+    }
   }
 }
 
@@ -1032,31 +1193,110 @@ enum SweepMode { SW_LUSGS_FWD = 0, SW_LUSGS_BWD = 1, SW_GS = 2 };
 
 // Neighbour contribution (add_nb / add_nb_contrib, StateUpdater.cpp:326-347, 401-426);
 // cn is the neighbour's compact index, km the current point's metrics for its direction.
-template <typename S, typename T, int MODE>
-__device__ __forceinline__ void sweep_nb(const BlockDev<S>& B, const ParamsDev& P, long long cn, const T km[3],
-                                         T sgn, T rhs0[5]) {
-  const long long nc = B.ncomp;
-  T pn[5], dn[5];
-  for (int m = 0; m < 5; ++m) {
-    pn[m] = (T)B.sk_prim[m * nc + cn];
-    dn[m] = (T)B.sk_dq[m * nc + cn];
+// All four sweeps in one persistent cooperative launch, software-pipelined.
+// Every CTA walks the hyperplane sequence; for each hyperplane a thread owns at
+// most one point of its CTA's first chunk (further chunks are handled in place).
+// The point's operands that do not change during the sweep (metrics, diagonal
+// coefficient, RHS or its own earlier increment, neighbour indices) are loaded
+// before the grid barrier that ends the previous hyperplane, so after the
+// barrier one round of independent L2 loads (the neighbours' state and fresh
+// increments) precedes the arithmetic.  The barrier's wait is bounded: after
+// spin_limit polls the kernel records an error and every CTA returns (the host
+// reports ORION_E_TIMEOUT) instead of spinning forever.
+struct SweepCtl {
+  unsigned int counter;
+  int error;
+};
+
+__device__ __forceinline__ bool grid_barrier(SweepCtl* ctl, unsigned int target, long long spin_limit) {
+  __syncthreads();
+  __shared__ int s_abort;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(&ctl->counter, 1u);
+    long long it = 0;
+    int abort = 0;
+    while (true) {
+      const unsigned int v = *(volatile unsigned int*)&ctl->counter;
+      if (v >= target) break;
+      if (*(volatile int*)&ctl->error) { abort = 1; break; }
+      if (++it > spin_limit) {
+        atomicExch(&ctl->error, 1);
+        abort = 1;
+        break;
+      }
+      __nanosleep(32);
+    }
+    __threadfence();
+    s_abort = abort;
   }
-  const T gamma = T(P.gamma);
-  const T r = spectral_radius<T>(pn[0], pn[1], pn[2], pn[3], pn[4], gamma, km[0], km[1], km[2]);
+  __syncthreads();
+  return s_abort == 0;
+}
+
+template <typename T>
+struct SweepOps {
+  int block;     // -1: no point
+  int c;         // compact index
+  int nb[6];     // neighbour compact indices: lower i,j,k then upper i,j,k; -1 outside the interior
+  T coed;
+  T own[5];      // -rhs (forward LU-SGS, GS) or the point's forward increment (backward LU-SGS)
+};
+
+template <typename S, typename T, int MODE>
+__device__ __forceinline__ void sweep_fetch(const BlockDev<S>& B, int block, int c, SweepOps<T>& o) {
+  const long long nc = B.ncomp;
+  o.block = block;
+  o.c = c;
+  for (int q = 0; q < 6; ++q) {
+    const bool used = (q < 3) ? (MODE == SW_LUSGS_FWD || MODE == SW_GS) : (MODE == SW_LUSGS_BWD || MODE == SW_GS);
+    o.nb[q] = used ? B.sk_nb[q * nc + c] : -1;
+  }
+  o.coed = (T)B.sk_coed[c];
+  for (int m = 0; m < 5; ++m) {
+    if (MODE == SW_LUSGS_BWD) o.own[m] = (T)__ldcg(B.sk_dq + m * nc + c);
+    else o.own[m] = -(T)B.sk_rhs[m * nc + c];
+  }
+}
+
+// The increment-dependent part of add_nb / add_nb_contrib for neighbour q
+// (compute_flux_splitting from dc on, StateUpdater.cpp:255-264, and the viscous
+// off-diagonal term :334-343 / :410-421), accumulated into rhs0 in the
+// reference's order.
+template <typename S, typename T, int MODE>
+__device__ __forceinline__ void sweep_term(const BlockDev<S>& B, T gm1, int nvis, const SweepOps<T>& o, int q,
+                                           T rhs0[5]) {
+  const long long nc = B.ncomp;
+  const long long n = o.nb[q];
+  const T drm = (T)__ldcg(B.sk_dq + n), dum = (T)__ldcg(B.sk_dq + nc + n), dvm = (T)__ldcg(B.sk_dq + 2 * nc + n),
+          dwm = (T)__ldcg(B.sk_dq + 3 * nc + n), dEm = (T)__ldcg(B.sk_dq + 4 * nc + n);
+  const T um = (T)B.sk_nbq[n], vm = (T)B.sk_nbq[nc + n], wm = (T)B.sk_nbq[2 * nc + n];
+  const T H = (T)B.sk_nbq[3 * nc + n], c2 = (T)B.sk_nbq[4 * nc + n], af = (T)B.sk_nbq[5 * nc + n];
+  const int d = q % 3;
+  const long long c = o.c;
+  const T nx_n = (T)B.sk_nrm[(3 * d) * nc + c], ny_n = (T)B.sk_nrm[(3 * d + 1) * nc + c],
+          nz_n = (T)B.sk_nrm[(3 * d + 2) * nc + c];
+  const S* pc = B.sk_pair + (long long)(5 * q) * nc + c;
+  const T l1 = (T)pc[0], x1 = (T)pc[nc], x2 = (T)pc[2 * nc], ct_n = (T)pc[3 * nc], rvh = (T)pc[4 * nc];
+  const T dc = ct_n * drm - (nx_n * dum + ny_n * dvm + nz_n * dwm);
+  const T dh = af * drm - gm1 * (um * dum + vm * dvm + wm * dwm - dEm);
+  const T c2dc = c2 * dc;
   T fs[5];
-  flux_split<T>(pn, dn, km[0], km[1], km[2], r, sgn, gamma, fs);
-  if (P.nvis == 1) {
-    const T mu_nb = (T)B.sk_mu[cn];
-    T vol_nb = (T)B.sk_vol[cn];
-    if (vol_nb < T(1e-30)) vol_nb = T(1e-30);
-    const T rv = visc_spectral_radius<T>(pn[0], mu_nb, vol_nb, T(P.reynolds), km[0], km[1], km[2]);
+  fs[0] = l1 * drm - dh * x1 - dc * x2;
+  fs[1] = l1 * dum + (nx_n * c2dc - um * dh) * x1 + (nx_n * dh - um * dc) * x2;
+  fs[2] = l1 * dvm + (ny_n * c2dc - vm * dh) * x1 + (ny_n * dh - vm * dc) * x2;
+  fs[3] = l1 * dwm + (nz_n * c2dc - wm * dh) * x1 + (nz_n * dh - wm * dc) * x2;
+  fs[4] = l1 * dEm + (ct_n * c2dc - H * dh) * x1 + (ct_n * dh - H * dc) * x2;
+  const T dn[5] = {drm, dum, dvm, dwm, dEm};
+  const T sgn = q < 3 ? T(1) : T(-1);
+  if (nvis == 1) {
     if (MODE == SW_GS) {
-      for (int m = 0; m < 5; ++m) fs[m] += T(0.5) * rv * dn[m] * sgn;
+      for (int m = 0; m < 5; ++m) fs[m] += rvh * dn[m] * sgn;
     } else {
-      for (int m = 0; m < 5; ++m) fs[m] += T(0.5) * rv * dn[m];
+      for (int m = 0; m < 5; ++m) fs[m] += rvh * dn[m];
     }
   }
-  if (MODE == SW_GS && sgn < T(0)) {
+  if (MODE == SW_GS && q >= 3) {
     for (int m = 0; m < 5; ++m) rhs0[m] -= fs[m];
   } else {
     for (int m = 0; m < 5; ++m) rhs0[m] += fs[m];
@@ -1064,50 +1304,270 @@ __device__ __forceinline__ void sweep_nb(const BlockDev<S>& B, const ParamsDev& 
 }
 
 template <typename S, typename T, int MODE>
-__device__ __forceinline__ void sweep_point(const BlockDev<S>& B, const ParamsDev& P, long long c) {
+__device__ __forceinline__ void sweep_apply(const BlockDev<S>& B, const ParamsDev& P, const SweepOps<T>& o) {
   const long long nc = B.ncomp;
-  int ii, jj, kk;
-  decode_nat(B, B.sk_nat[c], ii, jj, kk);
-  const int s = ii + jj + kk;
-  const int nk = B.nk;
-  T km[9];
-  for (int m = 0; m < 9; ++m) km[m] = (T)B.sk_metrics[m * nc + c];
+  const T gm1 = T(P.gamma) - T(1);
   T rhs0[5] = {T(0), T(0), T(0), T(0), T(0)};
-  if (MODE == SW_LUSGS_FWD || MODE == SW_GS) {
-    const int* ko = B.koff + (s - 1) * nk;
-    if (ii > 0) sweep_nb<S, T, MODE>(B, P, ko[kk] + (jj - jlo_of(B, s - 1, kk)), km + 0, T(1), rhs0);
-    if (jj > 0) sweep_nb<S, T, MODE>(B, P, ko[kk] + (jj - 1 - jlo_of(B, s - 1, kk)), km + 3, T(1), rhs0);
-    if (kk > 0) sweep_nb<S, T, MODE>(B, P, ko[kk - 1] + (jj - jlo_of(B, s - 1, kk - 1)), km + 6, T(1), rhs0);
-  }
-  if (MODE == SW_LUSGS_BWD || MODE == SW_GS) {
-    const int* ko = B.koff + (s + 1) * nk;
-    if (ii < B.ni - 1) sweep_nb<S, T, MODE>(B, P, ko[kk] + (jj - jlo_of(B, s + 1, kk)), km + 0, T(-1), rhs0);
-    if (jj < B.nj - 1) sweep_nb<S, T, MODE>(B, P, ko[kk] + (jj + 1 - jlo_of(B, s + 1, kk)), km + 3, T(-1), rhs0);
-    if (kk < B.nk - 1) sweep_nb<S, T, MODE>(B, P, ko[kk + 1] + (jj - jlo_of(B, s + 1, kk + 1)), km + 6, T(-1), rhs0);
-  }
-  const T coed = (T)B.sk_coed[c];
+  // lower neighbours first (i, j, k), then upper (i, j, k): the reference's order
+  for (int q = 0; q < 6; ++q)
+    if (o.nb[q] >= 0) sweep_term<S, T, MODE>(B, gm1, P.nvis, o, q, rhs0);
   for (int m = 0; m < 5; ++m) {
-    S* d = B.sk_dq + m * nc + c;
-    if (MODE == SW_LUSGS_FWD) {
-      const T explicit_term = -(T)B.sk_rhs[m * nc + c];
-      *d = (S)((explicit_term + rhs0[m]) * coed);
-    } else if (MODE == SW_LUSGS_BWD) {
-      *d = (S)((T)*d - rhs0[m] * coed);
-    } else {
-      const T resid = -(T)B.sk_rhs[m * nc + c];
-      *d = (S)((rhs0[m] + resid) * coed);
-    }
+    S* d = B.sk_dq + m * nc + o.c;
+    if (MODE == SW_LUSGS_FWD) *d = (S)((o.own[m] + rhs0[m]) * o.coed);
+    else if (MODE == SW_LUSGS_BWD) *d = (S)(o.own[m] - rhs0[m] * o.coed);
+    else *d = (S)((rhs0[m] + o.own[m]) * o.coed);
   }
 }
 
 // One hyperplane of one sweep for every block; chunks list contiguous compact ranges.
-template <typename S, typename T, int MODE>
-__global__ void __launch_bounds__(256) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
-                                                     const Chunk* __restrict__ chunks, ParamsDev P) {
+template <typename S, typename T, int MODE, int NT>
+__global__ void __launch_bounds__(NT) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
+                                                    const Chunk* __restrict__ chunks, ParamsDev P) {
   const Chunk ch = chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.count) return;
-  const BlockDev<S> B = blocks[ch.block];
-  sweep_point<S, T, MODE>(B, P, ch.start + threadIdx.x);
+  const BlockDev<S>& B = blocks[ch.block];
+  SweepOps<T> o;
+  sweep_fetch<S, T, MODE>(B, ch.block, (int)ch.start + threadIdx.x, o);
+  sweep_apply<S, T, MODE>(B, P, o);
+}
+
+template <typename S, typename T, int MODE>
+__device__ __forceinline__ bool persistent_pass(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks,
+                                                const int* __restrict__ off, int nlaunch, const ParamsDev& P,
+                                                SweepCtl* ctl, unsigned int& target, long long spin_limit) {
+  SweepOps<T> cur;
+  cur.block = -1;
+  // prefetch hyperplane 0
+  {
+    const int ci = off[0] + blockIdx.x;
+    if (ci < off[1]) {
+      const Chunk ch = chunks[ci];
+      if ((int)threadIdx.x < ch.count)
+        sweep_fetch<S, T, MODE>(blocks[ch.block], ch.block, (int)ch.start + threadIdx.x, cur);
+    }
+  }
+  for (int t = 0; t < nlaunch; ++t) {
+    if (cur.block >= 0) sweep_apply<S, T, MODE>(blocks[cur.block], P, cur);
+    // further chunks of this hyperplane owned by this CTA (large hyperplanes only)
+    for (int ci = off[t] + blockIdx.x + gridDim.x; ci < off[t + 1]; ci += gridDim.x) {
+      const Chunk ch = chunks[ci];
+      if ((int)threadIdx.x < ch.count) {
+        SweepOps<T> x;
+        sweep_fetch<S, T, MODE>(blocks[ch.block], ch.block, (int)ch.start + threadIdx.x, x);
+        sweep_apply<S, T, MODE>(blocks[ch.block], P, x);
+      }
+    }
+    // prefetch the next hyperplane's static operands, then wait for this one
+    cur.block = -1;
+    if (t + 1 < nlaunch) {
+      const int ci = off[t + 1] + blockIdx.x;
+      if (ci < off[t + 2]) {
+        const Chunk ch = chunks[ci];
+        if ((int)threadIdx.x < ch.count)
+          sweep_fetch<S, T, MODE>(blocks[ch.block], ch.block, (int)ch.start + threadIdx.x, cur);
+      }
+    }
+    target += gridDim.x;
+    if (!grid_barrier(ctl, target, spin_limit)) return false;
+  }
+  return true;
+}
+
+template <typename S, typename T, int NT>
+__global__ void __launch_bounds__(NT) k_sweeps_persistent(const BlockDev<S>* __restrict__ blocks,
+                                                           const Chunk* __restrict__ fwd_chunks,
+                                                           const int* __restrict__ fwd_off,
+                                                           const Chunk* __restrict__ bwd_chunks,
+                                                           const int* __restrict__ bwd_off, int nlaunch,
+                                                           ParamsDev P, SweepCtl* ctl, long long spin_limit) {
+  unsigned int target = 0;
+  if (!persistent_pass<S, T, SW_LUSGS_FWD>(blocks, fwd_chunks, fwd_off, nlaunch, P, ctl, target, spin_limit)) return;
+  if (!persistent_pass<S, T, SW_LUSGS_BWD>(blocks, bwd_chunks, bwd_off, nlaunch, P, ctl, target, spin_limit)) return;
+  if (!persistent_pass<S, T, SW_GS>(blocks, fwd_chunks, fwd_off, nlaunch, P, ctl, target, spin_limit)) return;
+  persistent_pass<S, T, SW_GS>(blocks, bwd_chunks, bwd_off, nlaunch, P, ctl, target, spin_limit);
+}
+
+// Cluster form of the four sweeps.  Mesh blocks are independent, so only the
+// CTAs that share a block have to agree on hyperplane boundaries: each thread
+// block cluster owns a group of mesh blocks and walks the hyperplanes of that
+// group, separating consecutive hyperplanes with the hardware cluster barrier
+// (release/acquire at cluster scope).  No cluster waits on another, so clusters
+// may also run one after another.  Software-pipelined like the persistent form.
+__device__ __forceinline__ void cluster_arrive() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+// The fields of a block the sweeps touch, staged in shared memory so no
+// hyperplane pays a global load for a pointer.
+template <typename S>
+struct SweepBlock {
+  S* dq;
+  const int* nb;
+  const S* coed;
+  const S* rhs;
+  const S* nbq;
+  const S* pair;
+  const S* nrm;
+  long long nc;
+};
+
+// A thread's share of one hyperplane: up to two chunks, staged per pass.
+struct SweepSlot {
+  int block;  // -1: none
+  int start;
+  int count;
+};
+
+template <typename S, typename T, int MODE>
+__device__ __forceinline__ void cl_fetch(const SweepBlock<S>& B, int block, int c, SweepOps<T>& o) {
+  const long long nc = B.nc;
+  o.block = block;
+  o.c = c;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    const bool used = (q < 3) ? (MODE == SW_LUSGS_FWD || MODE == SW_GS) : (MODE == SW_LUSGS_BWD || MODE == SW_GS);
+    o.nb[q] = used ? __ldg(B.nb + q * nc + c) : -1;
+  }
+  o.coed = (T)B.coed[c];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    if (MODE == SW_LUSGS_BWD) o.own[m] = (T)__ldcg(B.dq + m * nc + c);
+    else o.own[m] = -(T)B.rhs[m * nc + c];
+  }
+}
+
+template <typename S, typename T, int MODE>
+__device__ __forceinline__ void cl_term(const SweepBlock<S>& B, T gm1, int nvis, const SweepOps<T>& o, int q,
+                                        T rhs0[5]) {
+  const long long nc = B.nc;
+  const long long n = o.nb[q];
+  const T drm = (T)__ldcg(B.dq + n), dum = (T)__ldcg(B.dq + nc + n), dvm = (T)__ldcg(B.dq + 2 * nc + n),
+          dwm = (T)__ldcg(B.dq + 3 * nc + n), dEm = (T)__ldcg(B.dq + 4 * nc + n);
+  const T um = (T)B.nbq[n], vm = (T)B.nbq[nc + n], wm = (T)B.nbq[2 * nc + n];
+  const T H = (T)B.nbq[3 * nc + n], c2 = (T)B.nbq[4 * nc + n], af = (T)B.nbq[5 * nc + n];
+  const int d = q % 3;
+  const long long c = o.c;
+  const T nx_n = (T)B.nrm[(3 * d) * nc + c], ny_n = (T)B.nrm[(3 * d + 1) * nc + c], nz_n = (T)B.nrm[(3 * d + 2) * nc + c];
+  const S* pc = B.pair + (long long)(5 * q) * nc + c;
+  const T l1 = (T)pc[0], x1 = (T)pc[nc], x2 = (T)pc[2 * nc], ct_n = (T)pc[3 * nc], rvh = (T)pc[4 * nc];
+  // compute_flux_splitting from dc on (StateUpdater.cpp:255-264) + viscous term (:334-343 / :410-421)
+  const T dc = ct_n * drm - (nx_n * dum + ny_n * dvm + nz_n * dwm);
+  const T dh = af * drm - gm1 * (um * dum + vm * dvm + wm * dwm - dEm);
+  const T c2dc = c2 * dc;
+  T fs[5];
+  fs[0] = l1 * drm - dh * x1 - dc * x2;
+  fs[1] = l1 * dum + (nx_n * c2dc - um * dh) * x1 + (nx_n * dh - um * dc) * x2;
+  fs[2] = l1 * dvm + (ny_n * c2dc - vm * dh) * x1 + (ny_n * dh - vm * dc) * x2;
+  fs[3] = l1 * dwm + (nz_n * c2dc - wm * dh) * x1 + (nz_n * dh - wm * dc) * x2;
+  fs[4] = l1 * dEm + (ct_n * c2dc - H * dh) * x1 + (ct_n * dh - H * dc) * x2;
+  const T dn[5] = {drm, dum, dvm, dwm, dEm};
+  const T sgn = q < 3 ? T(1) : T(-1);
+  if (nvis == 1) {
+    if (MODE == SW_GS) {
+      for (int m = 0; m < 5; ++m) fs[m] += rvh * dn[m] * sgn;
+    } else {
+      for (int m = 0; m < 5; ++m) fs[m] += rvh * dn[m];
+    }
+  }
+  if (MODE == SW_GS && q >= 3) {
+    for (int m = 0; m < 5; ++m) rhs0[m] -= fs[m];
+  } else {
+    for (int m = 0; m < 5; ++m) rhs0[m] += fs[m];
+  }
+}
+
+template <typename S, typename T, int MODE>
+__device__ __forceinline__ void cl_apply(const SweepBlock<S>& B, T gm1, int nvis, const SweepOps<T>& o) {
+  const long long nc = B.nc;
+  T rhs0[5] = {T(0), T(0), T(0), T(0), T(0)};
+#pragma unroll
+  for (int q = 0; q < 6; ++q)
+    if (o.nb[q] >= 0) cl_term<S, T, MODE>(B, gm1, nvis, o, q, rhs0);
+  for (int m = 0; m < 5; ++m) {
+    S* d = B.dq + m * nc + o.c;
+    if (MODE == SW_LUSGS_FWD) *d = (S)((o.own[m] + rhs0[m]) * o.coed);
+    else if (MODE == SW_LUSGS_BWD) *d = (S)(o.own[m] - rhs0[m] * o.coed);
+    else *d = (S)((rhs0[m] + o.own[m]) * o.coed);
+  }
+}
+
+template <typename S, typename T, int MODE>
+__device__ __forceinline__ void cluster_pass(const SweepBlock<S>* sb, const Chunk* __restrict__ chunks,
+                                             const int* __restrict__ off, int nlaunch, int rank, int csize,
+                                             const ParamsDev& P, SweepSlot* slots) {
+  const T gm1 = T(P.gamma) - T(1);
+  // stage this CTA's chunk of every hyperplane (two per hyperplane)
+  __syncthreads();
+  for (int x = threadIdx.x; x < 2 * nlaunch; x += blockDim.x) {
+    const int t = x >> 1, r = x & 1;
+    const int ci = off[t] + rank + r * csize;
+    SweepSlot sl{-1, 0, 0};
+    if (ci < off[t + 1]) {
+      const Chunk ch = chunks[ci];
+      sl = SweepSlot{ch.block, (int)ch.start, ch.count};
+    }
+    slots[x] = sl;
+  }
+  __syncthreads();
+  SweepOps<T> cur[2];
+  auto fetch = [&](int t) {
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const SweepSlot sl = slots[2 * t + r];
+      cur[r].block = -1;
+      if (sl.block >= 0 && (int)threadIdx.x < sl.count)
+        cl_fetch<S, T, MODE>(sb[sl.block], sl.block, sl.start + threadIdx.x, cur[r]);
+    }
+  };
+  fetch(0);
+  for (int t = 0; t < nlaunch; ++t) {
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+      if (cur[r].block >= 0) cl_apply<S, T, MODE>(sb[cur[r].block], gm1, P.nvis, cur[r]);
+    // chunks beyond the two staged ones (very large hyperplanes only)
+    for (int ci = off[t] + rank + 2 * csize; ci < off[t + 1]; ci += csize) {
+      const Chunk ch = chunks[ci];
+      if ((int)threadIdx.x < ch.count) {
+        SweepOps<T> x;
+        cl_fetch<S, T, MODE>(sb[ch.block], ch.block, (int)ch.start + threadIdx.x, x);
+        cl_apply<S, T, MODE>(sb[ch.block], gm1, P.nvis, x);
+      }
+    }
+    // publish this hyperplane, fetch the next one's static operands, then wait
+    cluster_arrive();
+    if (t + 1 < nlaunch) fetch(t + 1);
+    cluster_wait();
+  }
+}
+
+template <typename S, typename T, int NT>
+__global__ void __launch_bounds__(NT, 1) k_sweeps_cluster(const BlockDev<S>* __restrict__ blocks, int nblocks,
+                                                          const Chunk* __restrict__ fwd_chunks,
+                                                          const int* __restrict__ fwd_off,
+                                                          const Chunk* __restrict__ bwd_chunks,
+                                                          const int* __restrict__ bwd_off,
+                                                          const int* __restrict__ grp_base,
+                                                          const int* __restrict__ grp_nplanes, ParamsDev P) {
+  namespace cg = cooperative_groups;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SweepBlock<S>* sb = reinterpret_cast<SweepBlock<S>*>(smem_raw);
+  SweepSlot* slots = reinterpret_cast<SweepSlot*>(smem_raw + sizeof(SweepBlock<S>) * nblocks);
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    const BlockDev<S>& B = blocks[b];
+    sb[b] = SweepBlock<S>{B.sk_dq, B.sk_nb, B.sk_coed, B.sk_rhs, B.sk_nbq, B.sk_pair, B.sk_nrm, B.ncomp};
+  }
+  cg::cluster_group cl = cg::this_cluster();
+  const int csize = (int)cl.num_blocks();
+  const int rank = (int)cl.block_rank();
+  const int g = blockIdx.x / csize;
+  const int base = grp_base[g], n = grp_nplanes[g];
+  cluster_pass<S, T, SW_LUSGS_FWD>(sb, fwd_chunks, fwd_off + base, n, rank, csize, P, slots);
+  cluster_pass<S, T, SW_LUSGS_BWD>(sb, bwd_chunks, bwd_off + base, n, rank, csize, P, slots);
+  cluster_pass<S, T, SW_GS>(sb, fwd_chunks, fwd_off + base, n, rank, csize, P, slots);
+  cluster_pass<S, T, SW_GS>(sb, bwd_chunks, bwd_off + base, n, rank, csize, P, slots);
 }
 
 // Finish: zero the physical-BC windows (set_boundary_dq_zero), scatter dq to
@@ -1263,7 +1723,8 @@ __global__ void __launch_bounds__(NT) k_update_res(const BlockDev<S>* __restrict
   long long key = (long long)0x7fffffffffffffffLL;
   for (int t = threadIdx.x; t < ch.count; t += NT) {
     const long long n = ch.start + t;
-    const int ii = (int)(n % B.ni), jj = (int)((n / B.ni) % B.nj), kk = (int)(n / ((long long)B.ni * B.nj));
+    const int n32 = (int)n, r32 = n32 / B.ni;
+    const int ii = n32 - r32 * B.ni, jj = r32 % B.nj, kk = r32 / B.nj;
     const long long idx = lin(B, NG + ii, NG + jj, NG + kk);
     double dq[5];
     if (DO_UPDATE && B.bcmask[idx]) {

@@ -10,96 +10,15 @@
 #include <string>
 #include <vector>
 
-#include "kernels.cuh"
-#include "orion_gpu.h"
-#include "topology.hpp"
+#include "case.hpp"
 
 using namespace orion;
 
-namespace {
-
-thread_local std::string g_last_error;
-
-int fail(int code, const std::string& msg) {
-  g_last_error = msg;
-  return code;
-}
-
-#define CUDA_TRY(expr)                                                                       \
-  do {                                                                                       \
-    cudaError_t _e = (expr);                                                                 \
-    if (_e != cudaSuccess)                                                                   \
-      return fail(ORION_E_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e));         \
-  } while (0)
-
-constexpr int kThreads = 256;
-constexpr int kChunk = 1024;        // points per CTA for pointwise kernels
-constexpr int kHistCap = 4096;      // residual history ring
-constexpr size_t kLineSmemBudget = 96 * 1024;
-
-size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-
-struct DeviceLists {
-  Chunk* pad_chunks = nullptr;
-  int n_pad_chunks = 0;
-  Chunk* int_chunks = nullptr;
-  int n_int_chunks = 0;
-  LineTile* tiles[3] = {nullptr, nullptr, nullptr};
-  int n_tiles[3] = {0, 0, 0};
-  int lanes[3] = {1, 1, 1};
-  int lmax[3] = {0, 0, 0};
-  Chunk* sweep_chunks[2] = {nullptr, nullptr};  // forward / backward hyperplane launches
-  std::vector<int> sweep_off[2];                 // host: chunk range of each launch
-  int max_planes = 0;
-  long long* halo_src = nullptr;
-  long long* halo_dst = nullptr;
-  int n_halo = 0;
-  RegionDev* regions = nullptr;
-  int* phase_regions = nullptr;
-  std::vector<int> phase_off;  // host: region list offsets per phase
-  std::vector<int> phase_maxpts;
-  int* pk_block = nullptr;
-  long long* pk_idx = nullptr;
-  double* pack = nullptr;
-  int n_pack = 0;
-  int* ap_block = nullptr;
-  long long* ap_idx = nullptr;
-  int* ap_off = nullptr;
-  int* ap_slot = nullptr;
-  int n_ap = 0;
-  ResPartial* partials = nullptr;
-  ResidualOut* hist = nullptr;
-  int* counter = nullptr;
-  unsigned long long* dtmin = nullptr;
-  long long* pad_base = nullptr;
-};
-
-}  // namespace
-
 namespace orion {
+thread_local std::string g_last_error;
 int set_error(int code, const std::string& msg) { return fail(code, msg); }
 }  // namespace orion
 
-struct orion_case_s {
-  int nblocks = 0;
-  int prec = ORION_PREC_FP64;
-  ParamsDev P{};
-  std::vector<HostBlock> hb;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  int device = 0;
-  void* arena = nullptr;
-  size_t arena_bytes = 0;
-  std::vector<void*> allocs;  // other device allocations
-  std::vector<BlockDev<double>> bd64;
-  std::vector<BlockDev<float>> bd32;
-  void* d_blocks = nullptr;
-  DeviceLists L;
-  long long total_interior = 0;
-  cudaGraphExec_t graph = nullptr;
-  long long steps_done = 0;
-  int step_launches = 0;
-};
 
 namespace {
 
@@ -144,7 +63,8 @@ size_t block_bytes(const HostBlock& b, size_t ssz) {
   const size_t npl = (size_t)(b.idim + b.jdim + b.kdim - 2);
   add((npl * b.kdim + 1) * 4);  // koff
   add(nc * 4);                  // sk_nat
-  add(27 * nc * ssz);           // sk_metrics 9, sk_vol, sk_prim 5, sk_mu, sk_coed, sk_rhs 5, sk_dq 5
+  add(6 * nc * 4);              // sk_nb
+  add(72 * nc * ssz);           // sk_metrics 9, sk_vol, sk_prim 5, sk_mu, sk_coed, sk_rhs 5, sk_dq 5, sk_nrm 9, sk_nbq 6, sk_pair 30
   return align_up(s, 256);
 }
 
@@ -174,7 +94,8 @@ void carve_block(char* base, const HostBlock& b, BlockDev<S>& d) {
   d.ncomp = (long long)nc;
   d.koff = reinterpret_cast<int*>(take(((size_t)npl * b.kdim + 1) * 4));
   d.sk_nat = reinterpret_cast<int*>(take(nc * 4));
-  S* sk = reinterpret_cast<S*>(take(27 * nc * sizeof(S)));
+  d.sk_nb = reinterpret_cast<int*>(take(6 * nc * 4));
+  S* sk = reinterpret_cast<S*>(take(72 * nc * sizeof(S)));
   d.sk_metrics = sk;
   d.sk_vol = sk + 9 * nc;
   d.sk_prim = sk + 10 * nc;
@@ -182,6 +103,9 @@ void carve_block(char* base, const HostBlock& b, BlockDev<S>& d) {
   d.sk_coed = sk + 16 * nc;
   d.sk_rhs = sk + 17 * nc;
   d.sk_dq = sk + 22 * nc;
+  d.sk_nrm = sk + 27 * nc;
+  d.sk_nbq = sk + 36 * nc;
+  d.sk_pair = sk + 42 * nc;
   d.ni = b.idim;
   d.nj = b.jdim;
   d.nk = b.kdim;
@@ -229,6 +153,91 @@ void plane_major_maps(const HostBlock& h, std::vector<int>& koff, std::vector<in
     }
   koff[(size_t)npl * nk] = (int)nat.size();
 }
+
+// Compact indices of the six face neighbours of every compact point (component
+// stride ncomp): lower i, j, k then upper i, j, k; -1 where the neighbour is a ghost.
+void plane_major_neighbours(const HostBlock& h, const std::vector<int>& koff, const std::vector<int>& nat,
+                            std::vector<int>& nb) {
+  const int ni = h.idim, nj = h.jdim, nk = h.kdim;
+  const size_t nc = nat.size();
+  nb.assign(6 * nc, -1);
+  auto jlo = [&](int s, int kk) { return std::max(0, s - kk - (ni - 1)); };
+  for (size_t c = 0; c < nc; ++c) {
+    const int v = nat[c];
+    const int i = v % h.nx, r = v / h.nx;
+    const int ii = i - NG, jj = r % h.ny - NG, kk = r / h.ny - NG;
+    const int s = ii + jj + kk;
+    if (ii > 0) nb[0 * nc + c] = koff[(size_t)(s - 1) * nk + kk] + (jj - jlo(s - 1, kk));
+    if (jj > 0) nb[1 * nc + c] = koff[(size_t)(s - 1) * nk + kk] + (jj - 1 - jlo(s - 1, kk));
+    if (kk > 0) nb[2 * nc + c] = koff[(size_t)(s - 1) * nk + kk - 1] + (jj - jlo(s - 1, kk - 1));
+    if (ii < ni - 1) nb[3 * nc + c] = koff[(size_t)(s + 1) * nk + kk] + (jj - jlo(s + 1, kk));
+    if (jj < nj - 1) nb[4 * nc + c] = koff[(size_t)(s + 1) * nk + kk] + (jj + 1 - jlo(s + 1, kk));
+    if (kk < nk - 1) nb[5 * nc + c] = koff[(size_t)(s + 1) * nk + kk + 1] + (jj - jlo(s + 1, kk + 1));
+  }
+}
+
+}  // namespace
+
+int orion::build_cluster_lists(orion_case_t c, int nclusters) {
+  auto& L = c->L;
+  const int nb = c->nblocks;
+  nclusters = std::max(1, std::min(nclusters, nb));
+  std::vector<int> order(nb);
+  for (int b = 0; b < nb; ++b) order[b] = b;
+  std::sort(order.begin(), order.end(), [&](int a, int b) {
+    const auto& ha = c->hb[a];
+    const auto& hb = c->hb[b];
+    return (long long)ha.idim * ha.jdim * ha.kdim > (long long)hb.idim * hb.jdim * hb.kdim;
+  });
+  std::vector<std::vector<int>> groups(nclusters);
+  std::vector<long long> load(nclusters, 0);
+  for (int b : order) {
+    const int g = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    groups[g].push_back(b);
+    load[g] += (long long)c->hb[b].idim * c->hb[b].jdim * c->hb[b].kdim;
+  }
+  std::vector<std::vector<int>> koffs(nb);
+  for (int b = 0; b < nb; ++b) {
+    std::vector<int> nat;
+    plane_major_maps(c->hb[b], koffs[b], nat);
+  }
+  const int nt = L.sweep_nt;
+  std::vector<int> base, npl;
+  for (int dir = 0; dir < 2; ++dir) {
+    std::vector<Chunk> ch;
+    std::vector<int> off;
+    base.clear();
+    npl.clear();
+    for (int g = 0; g < nclusters; ++g) {
+      int pmax = 0;
+      for (int b : groups[g]) pmax = std::max(pmax, c->hb[b].idim + c->hb[b].jdim + c->hb[b].kdim - 2);
+      base.push_back((int)off.size());
+      npl.push_back(pmax);
+      for (int t = 0; t < pmax; ++t) {
+        off.push_back((int)ch.size());
+        for (int b : groups[g]) {
+          const auto& h = c->hb[b];
+          const int np_b = h.idim + h.jdim + h.kdim - 2;
+          if (t >= np_b) continue;
+          const int sp = dir == 0 ? t : np_b - 1 - t;
+          const int lo = koffs[b][(size_t)sp * h.kdim], hi = koffs[b][(size_t)(sp + 1) * h.kdim];
+          for (int x = lo; x < hi; x += nt) ch.push_back(Chunk{b, std::min(nt, hi - x), (long long)x});
+        }
+      }
+      off.push_back((int)ch.size());
+    }
+    int rc;
+    if ((rc = dev_upload(c, &L.cl_chunks[dir], ch))) return rc;
+    if ((rc = dev_upload(c, &L.cl_off[dir], off))) return rc;
+  }
+  int rc;
+  if ((rc = dev_upload(c, &L.cl_base, base))) return rc;
+  if ((rc = dev_upload(c, &L.cl_nplanes, npl))) return rc;
+  L.cl_count = nclusters;
+  return 0;
+}
+
+namespace {
 
 // --------------------------------------------------------------------------
 // work-list builders
@@ -291,7 +300,14 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
       void* dn = b64 ? (void*)b64->sk_nat : (void*)b32->sk_nat;
       CUDA_TRY(cudaMemcpy(dk, koffs[b].data(), koffs[b].size() * 4, cudaMemcpyHostToDevice));
       CUDA_TRY(cudaMemcpy(dn, nat.data(), nat.size() * 4, cudaMemcpyHostToDevice));
+      std::vector<int> nbv;
+      plane_major_neighbours(h, koffs[b], nat, nbv);
+      void* dnb = b64 ? (void*)b64->sk_nb : (void*)b32->sk_nb;
+      CUDA_TRY(cudaMemcpy(dnb, nbv.data(), nbv.size() * 4, cudaMemcpyHostToDevice));
     }
+    // FP32 sweeps fit 512 threads per CTA without spilling, FP64 sweeps 256
+    const int nt = c->prec == ORION_PREC_FP64 ? 256 : 512;
+    L.sweep_nt = nt;
     for (int dir = 0; dir < 2; ++dir) {
       std::vector<Chunk> ch;
       std::vector<int> off{0};
@@ -302,11 +318,12 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
           if (t >= npl) continue;
           const int sp = dir == 0 ? t : npl - 1 - t;
           const int lo = koffs[b][(size_t)sp * h.kdim], hi = koffs[b][(size_t)(sp + 1) * h.kdim];
-          for (int x = lo; x < hi; x += kThreads) ch.push_back(Chunk{b, std::min(kThreads, hi - x), (long long)x});
+          for (int x = lo; x < hi; x += nt) ch.push_back(Chunk{b, std::min(nt, hi - x), (long long)x});
         }
         off.push_back((int)ch.size());
       }
       if ((rc = dev_upload(c, &L.sweep_chunks[dir], ch))) return rc;
+      if ((rc = dev_upload(c, &L.sweep_off_dev[dir], off))) return rc;
       L.sweep_off[dir] = off;
     }
   }
@@ -509,184 +526,21 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
   if ((rc = dev_alloc(c, &L.hist, (size_t)kHistCap))) return rc;
   if ((rc = dev_alloc(c, &L.counter, 1))) return rc;
   if ((rc = dev_alloc(c, &L.dtmin, 1))) return rc;
+  if ((rc = dev_alloc(c, &L.dt_part, (size_t)std::max(L.n_pad_chunks, L.n_int_chunks)))) return rc;
+  {
+    int* ctl = nullptr;
+    if ((rc = dev_alloc(c, &ctl, 4))) return rc;
+    L.sweep_ctl = ctl;
+  }
   return 0;
 }
 
-// --------------------------------------------------------------------------
-// stage launchers (templated on storage S and compute T)
-// --------------------------------------------------------------------------
-template <typename S, typename T>
-struct Stages {
-  static const BlockDev<S>* blocks(orion_case_t c) { return static_cast<const BlockDev<S>*>(c->d_blocks); }
+const StageOps& ops_for(int precision) { return precision == ORION_PREC_FP64 ? plain_ops() : mixed_ops(); }
 
-  // Line kernels take up to kLineSmemBudget of dynamic shared memory; the
-  // attribute is set once, before any stream capture.
-  static int set_attributes() {
-    const int b = (int)kLineSmemBudget;
-    CUDA_TRY(cudaFuncSetAttribute(k_viscous<0, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-    CUDA_TRY(cudaFuncSetAttribute(k_viscous<1, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-    CUDA_TRY(cudaFuncSetAttribute(k_viscous<2, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-    CUDA_TRY(cudaFuncSetAttribute(k_inviscid<0, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-    CUDA_TRY(cudaFuncSetAttribute(k_inviscid<1, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-    CUDA_TRY(cudaFuncSetAttribute(k_inviscid<2, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-    return 0;
-  }
-
-  static int exchange(orion_case_t c) {
-    auto& L = c->L;
-    if (L.n_halo > 0)
-      k_halo_copy<<<(L.n_halo + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(
-          static_cast<double*>(c->arena), L.halo_src, L.halo_dst, L.n_halo);
-    return 0;
-  }
-
-  static int bc(orion_case_t c) {
-    auto& L = c->L;
-    for (size_t p = 0; p + 1 < L.phase_off.size(); ++p) {
-      const int nr = L.phase_off[p + 1] - L.phase_off[p];
-      if (nr <= 0 || L.phase_maxpts[p] <= 0) continue;
-      dim3 grid((L.phase_maxpts[p] + kThreads - 1) / kThreads, nr);
-      k_bc_phase<S><<<grid, kThreads, 0, c->stream>>>(blocks(c), L.regions, L.phase_regions + L.phase_off[p], c->P);
-    }
-    return 0;
-  }
-
-  static int state(orion_case_t c, bool with_dt, bool with_q) {
-    auto& L = c->L;
-    if (with_dt) k_step_begin<<<1, 32, 0, c->stream>>>(L.dtmin);
-    if (with_dt && with_q)
-      k_state<S, true, true><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dtmin);
-    else if (with_dt)
-      k_state<S, false, true><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dtmin);
-    else if (with_q)
-      k_state<S, true, false><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dtmin);
-    else
-      k_state<S, false, false><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dtmin);
-    return 0;
-  }
-
-  static int timestep(orion_case_t c) {
-    auto& L = c->L;
-    k_step_begin<<<1, 32, 0, c->stream>>>(L.dtmin);
-    k_timestep<S><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P, L.dtmin);
-    return 0;
-  }
-
-  template <int D>
-  static void visc_dir(orion_case_t c) {
-    auto& L = c->L;
-    const size_t smem = (size_t)L.lanes[D] * (L.lmax[D] + 1) * 4 * sizeof(T);
-    k_viscous<D, S, T><<<L.n_tiles[D], kThreads, smem, c->stream>>>(blocks(c), L.tiles[D], c->P);
-  }
-
-  static int viscous(orion_case_t c) {
-    if (c->P.nvis != 1) return 0;
-    auto& L = c->L;
-    k_node_derivs<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks);
-    visc_dir<0>(c);
-    visc_dir<1>(c);
-    visc_dir<2>(c);
-    return 0;
-  }
-
-  template <int D>
-  static void inv_dir(orion_case_t c) {
-    auto& L = c->L;
-    const size_t smem = (size_t)L.lanes[D] * (L.lmax[D] + 1) * 5 * sizeof(T);
-    k_inviscid<D, S, T><<<L.n_tiles[D], kThreads, smem, c->stream>>>(blocks(c), L.tiles[D], c->P);
-  }
-
-  static int inviscid(orion_case_t c) {
-    inv_dir<0>(c);
-    inv_dir<1>(c);
-    inv_dir<2>(c);
-    return 0;
-  }
-
-  static int average(orion_case_t c) {
-    auto& L = c->L;
-    if (L.n_pack == 0) return 0;
-    k_iface_pack<S><<<(L.n_pack + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(blocks(c), L.pk_block, L.pk_idx,
-                                                                                       L.pack, L.n_pack);
-    k_iface_apply<S><<<(L.n_ap + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(
-        blocks(c), L.ap_block, L.ap_idx, L.ap_off, L.ap_slot, L.pack, L.n_ap);
-    return 0;
-  }
-
-  template <int MODE>
-  static void sweep(orion_case_t c, int dir) {
-    auto& L = c->L;
-    const auto& off = L.sweep_off[dir];
-    for (int t = 0; t + 1 < (int)off.size(); ++t) {
-      const int n = off[t + 1] - off[t];
-      if (n > 0) k_sweep_plane<S, T, MODE><<<n, kThreads, 0, c->stream>>>(blocks(c), L.sweep_chunks[dir] + off[t], c->P);
-    }
-  }
-
-  static int update(orion_case_t c, bool fuse_residual) {
-    auto& L = c->L;
-    k_lusgs_prep<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
-    sweep<SW_LUSGS_FWD>(c, 0);
-    sweep<SW_LUSGS_BWD>(c, 1);
-    sweep<SW_GS>(c, 0);
-    sweep<SW_GS>(c, 1);
-    if (fuse_residual) {
-      k_sweep_finish<S, true, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
-                                                                                     L.partials);
-      residual_final(c);
-    } else {
-      k_sweep_finish<S, false, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
-                                                                                      L.partials);
-    }
-    return 0;
-  }
-
-  static int skew_static(orion_case_t c, int b) {
-    k_skew_static<S><<<148 * 4, kThreads, 0, c->stream>>>(blocks(c), b);
-    return 0;
-  }
-
-  static void residual_final(orion_case_t c) {
-    auto& L = c->L;
-    k_res_final<S><<<1, 1024, 0, c->stream>>>(blocks(c), c->nblocks, L.partials, L.n_int_chunks, c->total_interior * 5,
-                                              L.dtmin, L.hist, L.counter, kHistCap);
-  }
-
-  static int residual(orion_case_t c) {
-    auto& L = c->L;
-    k_update_res<S, false, true, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
-                                                                                        L.partials);
-    residual_final(c);
-    return 0;
-  }
-
-  // One whole step in the order of OrionSolver::solve (OrionSolver.cpp:141-209).
-  static int step(orion_case_t c, bool with_q) {
-    exchange(c);
-    bc(c);
-    state(c, true, with_q);
-    viscous(c);
-    if (c->P.nvis == 1) average(c);
-    inviscid(c);
-    average(c);
-    update(c, true);
-    return 0;
-  }
-
-  static int init_flow(orion_case_t c, uint64_t seed, double amp) {
-    auto& L = c->L;
-    k_init_flow<S><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, L.pad_base, c->P, seed, amp);
-    return 0;
-  }
-};
-
-using Plain = Stages<double, double>;
-using Mixed = Stages<float, float>;
-
-template <typename F1, typename F2>
-int dispatch(orion_case_t c, F1 plain, F2 mixed) {
+template <typename F>
+int dispatch(orion_case_t c, F fn) {
   if (!c) return fail(ORION_E_INVALID, "null case");
-  int rc = (c->prec == ORION_PREC_FP64) ? plain() : mixed();
+  int rc = fn(ops_for(c->prec));
   if (rc) return rc;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(ORION_E_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
@@ -729,18 +583,31 @@ int field_info(orion_case_t c, int block, int field, void** dptr, int* ncomp, bo
 // ============================================================================
 // C ABI
 // ============================================================================
+static int capture_step(orion_case_t c, cudaGraph_t* g) {
+  CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = ops_for(c->prec).step(c, c->prec == ORION_PREC_FP64);
+  cudaError_t e = cudaStreamEndCapture(c->stream, g);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(ORION_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  return 0;
+}
+
 static int ensure_graph(orion_case_t c) {
   if (c->graph) return 0;
   cudaGraph_t g;
-  CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = (c->prec == ORION_PREC_FP64) ? Plain::step(c, true) : Mixed::step(c, false);
-  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  int rc = capture_step(c, &g);
+  if (rc && (c->L.persist_grid > 0 || c->L.cl_size > 0)) {
+    // the cluster / cooperative sweep launch could not be captured: per-hyperplane launches
+    cudaGetLastError();
+    c->L.persist_grid = 0;
+    c->L.cl_size = 0;
+    rc = capture_step(c, &g);
+  }
   if (rc) return rc;
-  if (e != cudaSuccess) return fail(ORION_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
   size_t nodes = 0;
   cudaGraphGetNodes(g, nullptr, &nodes);
   c->step_launches = (int)nodes;
-  e = cudaGraphInstantiate(&c->graph, g, 0);
+  cudaError_t e = cudaGraphInstantiate(&c->graph, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) {
     c->graph = nullptr;
@@ -895,7 +762,8 @@ int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion
     destroy_case(c.release());
     return rc;
   }
-  rc = (precision == ORION_PREC_FP64) ? Plain::set_attributes() : Mixed::set_attributes();
+  rc = ops_for(precision).set_attributes();
+  if (!rc) rc = ops_for(precision).persistent_grid(c.get());
   if (rc) {
     destroy_case(c.release());
     return rc;
@@ -953,6 +821,17 @@ int orion_case_step_launches(orion_case_t c, int* n) {
   return 0;
 }
 
+int orion_case_sweep_schedule(orion_case_t c, int out[5]) {
+  if (!c || !out) return fail(ORION_E_INVALID, "null argument");
+  const auto& L = c->L;
+  out[0] = L.cl_size > 0 ? 2 : (L.persist_grid > 0 ? 1 : 0);
+  out[1] = L.cl_size > 0 ? L.cl_count : L.persist_grid;
+  out[2] = L.cl_size;
+  out[3] = L.sweep_nt;
+  out[4] = L.max_planes;
+  return 0;
+}
+
 int orion_case_footprint(orion_case_t c, size_t* bytes) {
   if (!c || !bytes) return fail(ORION_E_INVALID, "null argument");
   *bytes = c->arena_bytes;
@@ -976,7 +855,7 @@ int orion_case_upload(orion_case_t c, int block, int field, const double* host) 
     CUDA_TRY(cudaMemcpy(d, host, n * sizeof(double), cudaMemcpyHostToDevice));
   }
   if (field == ORION_FIELD_METRICS || field == ORION_FIELD_VOL) {
-    rc = dispatch(c, [&] { return Plain::skew_static(c, block); }, [&] { return Mixed::skew_static(c, block); });
+    rc = dispatch(c, [&](const StageOps& o) { return o.skew_static(c, block); });
     if (rc) return rc;
     CUDA_TRY(cudaStreamSynchronize(c->stream));
   }
@@ -1003,32 +882,32 @@ int orion_case_download(orion_case_t c, int block, int field, double* host) {
 }
 
 int orion_case_init_flow(orion_case_t c, uint64_t seed, double amp) {
-  return dispatch(c, [&] { return Plain::init_flow(c, seed, amp); }, [&] { return Mixed::init_flow(c, seed, amp); });
+  return dispatch(c, [&](const StageOps& o) { return o.init_flow(c, seed, amp); });
 }
 
 int orion_exchange_bc(orion_case_t c) {
-  return dispatch(c, [&] { return Plain::exchange(c); }, [&] { return Mixed::exchange(c); });
+  return dispatch(c, [&](const StageOps& o) { return o.exchange(c); });
 }
 int orion_apply_physical_bc(orion_case_t c) {
-  return dispatch(c, [&] { return Plain::bc(c); }, [&] { return Mixed::bc(c); });
+  return dispatch(c, [&](const StageOps& o) { return o.bc(c); });
 }
 int orion_update_flow_states(orion_case_t c) {
-  return dispatch(c, [&] { return Plain::state(c, false, true); }, [&] { return Mixed::state(c, false, true); });
+  return dispatch(c, [&](const StageOps& o) { return o.state(c, false, true); });
 }
 int orion_calculate_time_step(orion_case_t c) {
-  return dispatch(c, [&] { return Plain::timestep(c); }, [&] { return Mixed::timestep(c); });
+  return dispatch(c, [&](const StageOps& o) { return o.timestep(c); });
 }
 int orion_compute_viscous_rhs(orion_case_t c) {
-  return dispatch(c, [&] { return Plain::viscous(c); }, [&] { return Mixed::viscous(c); });
+  return dispatch(c, [&](const StageOps& o) { return o.viscous(c); });
 }
 int orion_average_interface_residuals(orion_case_t c) {
-  return dispatch(c, [&] { return Plain::average(c); }, [&] { return Mixed::average(c); });
+  return dispatch(c, [&](const StageOps& o) { return o.average(c); });
 }
 int orion_compute_inviscid_rhs(orion_case_t c) {
-  return dispatch(c, [&] { return Plain::inviscid(c); }, [&] { return Mixed::inviscid(c); });
+  return dispatch(c, [&](const StageOps& o) { return o.inviscid(c); });
 }
 int orion_update_solution(orion_case_t c) {
-  return dispatch(c, [&] { return Plain::update(c, false); }, [&] { return Mixed::update(c, false); });
+  return dispatch(c, [&](const StageOps& o) { return o.update(c, false); });
 }
 
 static int read_hist(orion_case_t c, long long first, int n, orion_residual_t* out) {
@@ -1051,7 +930,7 @@ int orion_residual_compute(orion_case_t c, orion_residual_t* out) {
   int cnt = 0;
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   CUDA_TRY(cudaMemcpy(&cnt, c->L.counter, sizeof(int), cudaMemcpyDeviceToHost));
-  int rc = dispatch(c, [&] { return Plain::residual(c); }, [&] { return Mixed::residual(c); });
+  int rc = dispatch(c, [&](const StageOps& o) { return o.residual(c); });
   if (rc) return rc;
   return read_hist(c, cnt, 1, out);
 }
@@ -1087,6 +966,14 @@ int orion_step(orion_case_t c, int nsteps, orion_residual_t* hist) {
     int rc = orion_step_async(c, n);
     if (rc) return rc;
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (c->L.sweep_ctl) {
+      int ctl[2] = {0, 0};
+      CUDA_TRY(cudaMemcpy(ctl, c->L.sweep_ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
+      if (ctl[1]) {
+        CUDA_TRY(cudaMemset(c->L.sweep_ctl, 0, sizeof(ctl)));
+        return fail(ORION_E_TIMEOUT, "a grid barrier of the implicit sweeps gave up waiting");
+      }
+    }
     if (hist) {
       rc = read_hist(c, (long long)cnt + done, n, hist + done);
       if (rc) return rc;

@@ -1,0 +1,336 @@
+// Stage launchers, templated on storage S and compute T.  Included by exactly
+// one translation unit per precision.
+#pragma once
+#include <cstdlib>
+
+#include "case.hpp"
+#include "kernels.cuh"
+
+namespace orion {
+
+// --------------------------------------------------------------------------
+// stage launchers (templated on storage S and compute T)
+// --------------------------------------------------------------------------
+template <typename S, typename T>
+struct Stages {
+  static const BlockDev<S>* blocks(orion_case_t c) { return static_cast<const BlockDev<S>*>(c->d_blocks); }
+
+  // Line kernels take up to kLineSmemBudget of dynamic shared memory; the
+  // attribute is set once, before any stream capture.
+  static int set_attributes() {
+    const int b = (int)kLineSmemBudget;
+    CUDA_TRY(cudaFuncSetAttribute(k_viscous<0, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CUDA_TRY(cudaFuncSetAttribute(k_viscous<1, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CUDA_TRY(cudaFuncSetAttribute(k_viscous<2, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CUDA_TRY(cudaFuncSetAttribute(k_inviscid<0, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CUDA_TRY(cudaFuncSetAttribute(k_inviscid<1, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CUDA_TRY(cudaFuncSetAttribute(k_inviscid<2, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    return 0;
+  }
+
+  static int exchange(orion_case_t c) {
+    auto& L = c->L;
+    if (L.n_halo > 0)
+      k_halo_copy<<<(L.n_halo + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(
+          static_cast<double*>(c->arena), L.halo_src, L.halo_dst, L.n_halo);
+    return 0;
+  }
+
+  static int bc(orion_case_t c) {
+    auto& L = c->L;
+    for (size_t p = 0; p + 1 < L.phase_off.size(); ++p) {
+      const int nr = L.phase_off[p + 1] - L.phase_off[p];
+      if (nr <= 0 || L.phase_maxpts[p] <= 0) continue;
+      dim3 grid((L.phase_maxpts[p] + kThreads - 1) / kThreads, nr);
+      k_bc_phase<S><<<grid, kThreads, 0, c->stream>>>(blocks(c), L.regions, L.phase_regions + L.phase_off[p], c->P);
+    }
+    return 0;
+  }
+
+  static int state(orion_case_t c, bool with_dt, bool with_q) {
+    auto& L = c->L;
+    if (with_dt && with_q)
+      k_state<S, true, true><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dt_part);
+    else if (with_dt)
+      k_state<S, false, true><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dt_part);
+    else if (with_q)
+      k_state<S, true, false><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dt_part);
+    else
+      k_state<S, false, false><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dt_part);
+    if (with_dt) k_dtmin_final<<<1, 1024, 0, c->stream>>>(L.dt_part, L.n_pad_chunks, L.dtmin);
+    return 0;
+  }
+
+  static int timestep(orion_case_t c) {
+    auto& L = c->L;
+    k_timestep<S><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P, L.dt_part);
+    k_dtmin_final<<<1, 1024, 0, c->stream>>>(L.dt_part, L.n_int_chunks, L.dtmin);
+    return 0;
+  }
+
+  template <int D>
+  static void visc_dir(orion_case_t c) {
+    auto& L = c->L;
+    const size_t smem = (size_t)L.lanes[D] * (L.lmax[D] + 1) * 4 * sizeof(T);
+    k_viscous<D, S, T><<<L.n_tiles[D], kThreads, smem, c->stream>>>(blocks(c), L.tiles[D], c->P);
+  }
+
+  static int viscous(orion_case_t c) {
+    if (c->P.nvis != 1) return 0;
+    auto& L = c->L;
+    k_node_derivs<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks);
+    visc_dir<0>(c);
+    visc_dir<1>(c);
+    visc_dir<2>(c);
+    return 0;
+  }
+
+  template <int D>
+  static void inv_dir(orion_case_t c) {
+    auto& L = c->L;
+    const size_t smem = (size_t)L.lanes[D] * (L.lmax[D] + 1) * 5 * sizeof(T);
+    k_inviscid<D, S, T><<<L.n_tiles[D], kThreads, smem, c->stream>>>(blocks(c), L.tiles[D], c->P);
+  }
+
+  static int inviscid(orion_case_t c) {
+    inv_dir<0>(c);
+    inv_dir<1>(c);
+    inv_dir<2>(c);
+    return 0;
+  }
+
+  static int average(orion_case_t c) {
+    auto& L = c->L;
+    if (L.n_pack == 0) return 0;
+    k_iface_pack<S><<<(L.n_pack + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(blocks(c), L.pk_block, L.pk_idx,
+                                                                                       L.pack, L.n_pack);
+    k_iface_apply<S><<<(L.n_ap + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(
+        blocks(c), L.ap_block, L.ap_idx, L.ap_off, L.ap_slot, L.pack, L.n_ap);
+    return 0;
+  }
+
+  template <int MODE>
+  static void sweep(orion_case_t c, int dir) {
+    auto& L = c->L;
+    const auto& off = L.sweep_off[dir];
+    for (int t = 0; t + 1 < (int)off.size(); ++t) {
+      const int n = off[t + 1] - off[t];
+      if (n <= 0) continue;
+      if (L.sweep_nt == 512)
+        k_sweep_plane<S, T, MODE, 512><<<n, 512, 0, c->stream>>>(blocks(c), L.sweep_chunks[dir] + off[t], c->P);
+      else
+        k_sweep_plane<S, T, MODE, 256><<<n, 256, 0, c->stream>>>(blocks(c), L.sweep_chunks[dir] + off[t], c->P);
+    }
+  }
+
+  // Sweep scheduling.  Preferred: cluster sweeps (16- or 8-CTA clusters, as
+  // many as are co-resident, mesh blocks grouped per cluster).  Otherwise the
+  // persistent cooperative kernel, otherwise one launch per hyperplane.
+  // ORION_SWEEP=planes|grid|cluster selects one explicitly.
+  static size_t cluster_smem(orion_case_t c) {
+    return sizeof(SweepBlock<S>) * c->nblocks + sizeof(SweepSlot) * 2 * (size_t)c->L.max_planes;
+  }
+
+  template <int NT>
+  static int cluster_setup(orion_case_t c) {
+    auto kern = k_sweeps_cluster<S, T, NT>;
+    const size_t smem = cluster_smem(c);
+    if (smem > 200 * 1024) return 0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    for (int cs : {16, 8}) {
+      if (cs > 8 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        continue;
+      }
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(cs * 64);
+      cfg.blockDim = dim3(NT);
+      cfg.dynamicSmemBytes = smem;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = cs;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int ncl = 0;
+      if (cudaOccupancyMaxActiveClusters(&ncl, kern, &cfg) != cudaSuccess || ncl < 1) {
+        cudaGetLastError();
+        continue;
+      }
+      int rc = build_cluster_lists(c, ncl);
+      if (rc) return rc;
+      c->L.cl_size = cs;
+      return 0;
+    }
+    return 0;
+  }
+
+  static int persistent_grid(orion_case_t c) {
+    c->L.persist_grid = 0;
+    c->L.cl_size = 0;
+    // default: clusters for FP32 (co-resident 16-CTA clusters hold 8k threads),
+    // the cooperative grid for FP64 (clusters of 256-thread CTAs hold too few)
+    const char* env = getenv("ORION_SWEEP");
+    const std::string mode = env ? std::string(env) : std::string(sizeof(S) == 4 ? "cluster" : "grid");
+    if (mode == "planes") return 0;
+    const char* lim = getenv("ORION_SWEEP_SPIN_LIMIT");
+    if (lim) c->L.spin_limit = atoll(lim);
+    const int nt = c->L.sweep_nt;
+    if (mode == "cluster") {
+      int rc = nt == 512 ? cluster_setup<512>(c) : cluster_setup<256>(c);
+      if (rc) return rc;
+      if (c->L.cl_size > 0) return 0;
+    }
+    int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    if (nt == 512)
+      CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweeps_persistent<S, T, 512>, 512, 0));
+    else
+      CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweeps_persistent<S, T, 256>, 256, 0));
+    const int want = 512 / nt;
+    if (!coop || per_sm < want) return 0;
+    c->L.persist_grid = nsm * want;
+    return 0;
+  }
+
+  template <int NT>
+  static int sweeps_cluster_nt(orion_case_t c) {
+    auto& L = c->L;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(L.cl_count * L.cl_size);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = cluster_smem(c);
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = L.cl_size;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweeps_cluster<S, T, NT>, blocks(c), c->nblocks, (const Chunk*)L.cl_chunks[0],
+                                (const int*)L.cl_off[0], (const Chunk*)L.cl_chunks[1], (const int*)L.cl_off[1],
+                                (const int*)L.cl_base, (const int*)L.cl_nplanes, c->P));
+    return 0;
+  }
+
+  static int sweeps_persistent(orion_case_t c) {
+    auto& L = c->L;
+    SweepCtl* ctl = static_cast<SweepCtl*>(L.sweep_ctl);
+    CUDA_TRY(cudaMemsetAsync(&ctl->counter, 0, sizeof(unsigned int), c->stream));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(L.persist_grid);
+    cfg.blockDim = dim3(L.sweep_nt);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const long long spin_limit = L.spin_limit;
+    if (L.sweep_nt == 512)
+      CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweeps_persistent<S, T, 512>, blocks(c), (const Chunk*)L.sweep_chunks[0],
+                                  (const int*)L.sweep_off_dev[0], (const Chunk*)L.sweep_chunks[1],
+                                  (const int*)L.sweep_off_dev[1], L.max_planes, c->P, ctl, spin_limit));
+    else
+      CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweeps_persistent<S, T, 256>, blocks(c), (const Chunk*)L.sweep_chunks[0],
+                                  (const int*)L.sweep_off_dev[0], (const Chunk*)L.sweep_chunks[1],
+                                  (const int*)L.sweep_off_dev[1], L.max_planes, c->P, ctl, spin_limit));
+    return 0;
+  }
+
+  static int update(orion_case_t c, bool fuse_residual) {
+    auto& L = c->L;
+    k_lusgs_prep<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
+    k_sweep_pairs<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
+    if (L.cl_size > 0) {
+      int rc = L.sweep_nt == 512 ? sweeps_cluster_nt<512>(c) : sweeps_cluster_nt<256>(c);
+      if (rc) return rc;
+    } else if (L.persist_grid > 0) {
+      int rc = sweeps_persistent(c);
+      if (rc) return rc;
+    } else {
+      sweep<SW_LUSGS_FWD>(c, 0);
+      sweep<SW_LUSGS_BWD>(c, 1);
+      sweep<SW_GS>(c, 0);
+      sweep<SW_GS>(c, 1);
+    }
+    if (fuse_residual) {
+      k_sweep_finish<S, true, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
+                                                                                     L.partials);
+      residual_final(c);
+    } else {
+      k_sweep_finish<S, false, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
+                                                                                      L.partials);
+    }
+    return 0;
+  }
+
+  static int skew_static(orion_case_t c, int b) {
+    k_skew_static<S><<<148 * 4, kThreads, 0, c->stream>>>(blocks(c), b);
+    return 0;
+  }
+
+  static void residual_final(orion_case_t c) {
+    auto& L = c->L;
+    k_res_final<S><<<1, 1024, 0, c->stream>>>(blocks(c), c->nblocks, L.partials, L.n_int_chunks, c->total_interior * 5,
+                                              L.dtmin, L.hist, L.counter, kHistCap);
+  }
+
+  static int residual(orion_case_t c) {
+    auto& L = c->L;
+    k_update_res<S, false, true, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
+                                                                                        L.partials);
+    residual_final(c);
+    return 0;
+  }
+
+  // One whole step in the order of OrionSolver::solve (OrionSolver.cpp:141-209).
+  static int step(orion_case_t c, bool with_q) {
+    exchange(c);
+    bc(c);
+    state(c, true, with_q);
+    viscous(c);
+    if (c->P.nvis == 1) average(c);
+    inviscid(c);
+    average(c);
+    update(c, true);
+    return 0;
+  }
+
+  static int init_flow(orion_case_t c, uint64_t seed, double amp) {
+    auto& L = c->L;
+    k_init_flow<S><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, L.pad_base, c->P, seed, amp);
+    return 0;
+  }
+};
+
+template <typename S, typename T>
+StageOps make_ops() {
+  using X = Stages<S, T>;
+  StageOps o;
+  o.set_attributes = &X::set_attributes;
+  o.exchange = &X::exchange;
+  o.bc = &X::bc;
+  o.state = &X::state;
+  o.timestep = &X::timestep;
+  o.viscous = &X::viscous;
+  o.average = &X::average;
+  o.inviscid = &X::inviscid;
+  o.update = &X::update;
+  o.residual = &X::residual;
+  o.step = &X::step;
+  o.init_flow = &X::init_flow;
+  o.skew_static = &X::skew_static;
+  o.persistent_grid = &X::persistent_grid;
+  return o;
+}
+
+}  // namespace orion

@@ -142,6 +142,12 @@ class FlowFieldSet:
         check(_lib.load().orion_case_step_launches(self._h, C.byref(v)))
         return int(v.value)
 
+    def sweep_schedule(self) -> dict:
+        v = (C.c_int * 5)()
+        check(_lib.load().orion_case_sweep_schedule(self._h, v))
+        mode = {0: "planes", 1: "grid", 2: "cluster"}[v[0]]
+        return {"mode": mode, "units": v[1], "cluster_size": v[2], "threads": v[3], "hyperplanes": v[4]}
+
     def footprint(self) -> int:
         v = C.c_size_t()
         check(_lib.load().orion_case_footprint(self._h, C.byref(v)))
