@@ -202,29 +202,12 @@ def main():
         return
 
     import torch
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-
-    from orion_b200 import _lib, solver
+    from orion_b200 import _lib, replicas, solver
+    rep = replicas.from_env()
     K, W = args.steps, args.warmup
     npts = case.npoints
     metrics = [solver.grid_metrics(b, case.params.gcl) for b in case.blocks]
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = rep.barrier, rep.max_over_ranks
 
     def timed_steps(fs, nsteps):
         s = torch.cuda.ExternalStream(fs.stream_ptr())
@@ -258,8 +241,8 @@ def main():
     l2 = (num / den) ** 0.5
     per_rank_pts = npts * K
     mixed_ms, plain_ms = results["mixed"]["ms"], results["plain"]["ms"]
-    value = world * per_rank_pts / (mixed_ms / 1e3)
-    plain_value = world * per_rank_pts / (plain_ms / 1e3)
+    value = rep.aggregate_rate(per_rank_pts, mixed_ms / 1e3)
+    plain_value = rep.aggregate_rate(per_rank_pts, plain_ms / 1e3)
 
     # per-stage timing of one step on the mixed case -> dominant stage roofline
     fsm = results["mixed"]["fs"]
@@ -326,7 +309,7 @@ def main():
             _lib.check(lib.orion_case_download(fse.handle, b, _lib.FIELD_PRIM, C.c_void_p(t.data_ptr())))
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = world * npts * ne / e2e_s
+    e2e_value = rep.aggregate_rate(npts * ne, e2e_s)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -359,9 +342,7 @@ def main():
         print(json.dumps(line))
     for r in results.values():
         r["fs"].close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
 
 
 if __name__ == "__main__":
