@@ -117,6 +117,10 @@ int orion_gpu_init(int device);
 int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion_params_t* params,
                       int precision, orion_case_t* out);
 int orion_case_destroy(orion_case_t c);
+/* Replaces the case's parameters (the reference passes core::Params to every
+ * stage call, InviscidFluxComputer.hpp:17-18 and the others); takes effect
+ * from the next launch, the captured step graph is rebuilt. */
+int orion_case_set_params(orion_case_t c, const orion_params_t* params);
 /* Optional: run on a caller-provided cudaStream_t (passed as void*); NULL = the case's own stream. */
 int orion_case_set_stream(orion_case_t c, void* stream);
 int orion_case_sync(orion_case_t c);

@@ -45,6 +45,9 @@
 #include "solver/ResidualMonitor.hpp"
 #include "solver/StateUpdater.hpp"
 #include "solver/TimeIntegrator.hpp"
+#ifdef ORION_SHIM
+#include "orion_backend_cuda.hpp"
+#endif
 
 using namespace orion;
 
@@ -114,7 +117,16 @@ int main(int argc, char** argv) {
     if (s == "--snap-step" && a + 1 < argc) snap_step = std::atoi(argv[++a]);
     else if (s == "--time-only") time_only = true;
     else if (s == "--warmup" && a + 1 < argc) warmup = std::atoi(argv[++a]);
+#ifdef ORION_SHIM
+    else if (s == "--resident") orion::gpu::set_residency(orion::gpu::Residency::Resident);
+    else if (s == "--mixed") orion::gpu::set_mixed_precision(true);
+#endif
   }
+#ifdef ORION_SHIM
+  // The same driver over the B200 path: the solver classes resolve to
+  // orion_b200/shim/orion_backend_cuda.cpp instead of the reference's TUs.
+  backend_cuda_init();
+#endif
 
   core::Runtime::init(argc, argv);
 
@@ -166,6 +178,9 @@ int main(int argc, char** argv) {
   hist.reserve((size_t)nsteps * 8);
 
   auto snap = [&](int step, const char* name) {
+#ifdef ORION_SHIM
+    if (step == snap_step) orion::gpu::sync_to_host(fs);
+#endif
     if (step == snap_step) dump_state(out + "/snap_" + std::to_string(step) + "_" + name + ".bin", fs, params.step.phydtime);
   };
 
@@ -209,6 +224,9 @@ int main(int argc, char** argv) {
     f.write(reinterpret_cast<const char*>(&n), sizeof(n));
     f.write(reinterpret_cast<const char*>(hist.data()), (std::streamsize)(hist.size() * sizeof(double)));
   }
+#ifdef ORION_SHIM
+  orion::gpu::sync_to_host(fs);
+#endif
   if (!time_only) dump_state(out + "/final.bin", fs, params.step.phydtime);
 
   long long pts = 0;

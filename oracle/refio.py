@@ -20,6 +20,9 @@ FIELDS = (("prim", 6), ("q", 5), ("dq", 5), ("metrics", 9), ("vol", 1), ("dt", 1
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_HARNESS = os.path.join(HERE, "_ref", "orion_ref_harness")
+# The same driver source linked against the B200 path through the C++ drop-in
+# layer (make -C oracle shim); it is the product under test, not the oracle.
+SHIM_HARNESS = os.path.join(HERE, "_ref", "orion_shim_harness")
 
 
 def read_state(path: str) -> Dict:
@@ -66,3 +69,14 @@ def run_reference(case_dir: str, nsteps: int, out_dir: str, snap_step: int = -1,
 
 def reference_available() -> bool:
     return os.path.exists(REF_HARNESS)
+
+
+def run_shim(case_dir: str, nsteps: int, out_dir: str, extra=()) -> str:
+    os.makedirs(out_dir, exist_ok=True)
+    r = subprocess.run([SHIM_HARNESS, case_dir, str(nsteps), out_dir, *extra], check=True, capture_output=True,
+                       text=True)
+    return r.stdout
+
+
+def shim_available() -> bool:
+    return os.path.exists(SHIM_HARNESS)

@@ -617,6 +617,26 @@ static int ensure_graph(orion_case_t c) {
 }
 
 
+static void set_params_dev(ParamsDev& P, const orion_params_t& p) {
+  P.gamma = p.gamma;
+  P.moo = p.moo;
+  P.reynolds = p.reynolds;
+  P.prl = p.prl;
+  P.cfl = p.cfl;
+  P.twall = p.twall;
+  P.tref = p.tref;
+  P.visc = p.visc;
+  P.roo = p.roo;
+  P.uoo = p.uoo;
+  P.voo = p.voo;
+  P.woo = p.woo;
+  P.poo = p.poo;
+  P.too = p.too;
+  P.csrv = (double)p.csrv;
+  P.nvis = p.nvis;
+  P.method = p.method;
+}
+
 extern "C" {
 
 const char* orion_last_error(void) { return g_last_error.c_str(); }
@@ -662,24 +682,7 @@ int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion
   c->nblocks = nblocks;
   c->prec = precision;
   CUDA_TRY(cudaGetDevice(&c->device));
-  auto& P = c->P;
-  P.gamma = params->gamma;
-  P.moo = params->moo;
-  P.reynolds = params->reynolds;
-  P.prl = params->prl;
-  P.cfl = params->cfl;
-  P.twall = params->twall;
-  P.tref = params->tref;
-  P.visc = params->visc;
-  P.roo = params->roo;
-  P.uoo = params->uoo;
-  P.voo = params->voo;
-  P.woo = params->woo;
-  P.poo = params->poo;
-  P.too = params->too;
-  P.csrv = (double)params->csrv;
-  P.nvis = params->nvis;
-  P.method = params->method;
+  set_params_dev(c->P, *params);
 
   c->hb.resize(nblocks);
   long long tot = 0;
@@ -795,6 +798,16 @@ int orion_case_set_stream(orion_case_t c, void* stream) {
     c->own_stream = true;
   }
   if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return 0;
+}
+
+int orion_case_set_params(orion_case_t c, const orion_params_t* params) {
+  if (!c || !params) return fail(ORION_E_INVALID, "null argument");
+  set_params_dev(c->P, *params);
+  if (c->graph) {  // the captured step holds the old values: capture again on the next step
     cudaGraphExecDestroy(c->graph);
     c->graph = nullptr;
   }
