@@ -177,6 +177,20 @@ int orion_step_async(orion_case_t c, int nsteps);
 /* Copies the residual of the most recent step (waits). */
 int orion_last_residual(orion_case_t c, orion_residual_t* out);
 
+/* Non-blocking stepping for request loops that keep many cases in flight.
+ * orion_step_submit enqueues nsteps whole steps on the case's stream and an
+ * asynchronous copy of their residual history (the per-step
+ * ResidualMonitor::compute result, ResidualMonitor.hpp:20-21) into a pinned
+ * ring the case owns, and returns at once.  At most 4096 steps may be
+ * submitted and not yet polled.  The first call on a case waits once to read
+ * the device's step counter.
+ * orion_case_poll returns 0 while submitted steps are still running, and 1
+ * when the case's stream is idle, after copying up to cap of the finished
+ * steps' history entries, oldest first, to out (*n of them; the rest stay for
+ * the next poll).  It never waits. */
+int orion_step_submit(orion_case_t c, int nsteps);
+int orion_case_poll(orion_case_t c, orion_residual_t* out, int cap, int* n);
+
 /* Allocation-free residual norm of one block ------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * where they need the residual (a solver that reserves its whole device budget

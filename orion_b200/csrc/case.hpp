@@ -104,6 +104,11 @@ struct orion_case_s {
   cudaGraphExec_t graph = nullptr;
   long long steps_done = 0;
   int step_launches = 0;
+  // submitted steps whose history has not been polled (orion_step_submit / orion_case_poll)
+  orion::ResidualOut* hist_host = nullptr;  // pinned mirror of the device history ring
+  long long hist_count = -1;                // device history counter; -1 = not known on the host
+  long long pending_first = 0;
+  int pending_n = 0;
 };
 
 namespace orion {

@@ -8,6 +8,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include "case.hpp"
@@ -27,9 +28,10 @@ int dev_upload(orion_case_t c, T** dptr, const std::vector<T>& v) {
   *dptr = nullptr;
   if (v.empty()) return 0;
   void* p = nullptr;
-  if (cudaMalloc(&p, v.size() * sizeof(T)) != cudaSuccess) return fail(ORION_E_NOMEM, "cudaMalloc (work list)");
+  if (cudaMallocAsync(&p, v.size() * sizeof(T), c->stream) != cudaSuccess)
+    return fail(ORION_E_NOMEM, "cudaMallocAsync (work list)");
   c->allocs.push_back(p);
-  CUDA_TRY(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
   *dptr = static_cast<T*>(p);
   return 0;
 }
@@ -37,9 +39,10 @@ int dev_upload(orion_case_t c, T** dptr, const std::vector<T>& v) {
 template <typename T>
 int dev_alloc(orion_case_t c, T** dptr, size_t n) {
   void* p = nullptr;
-  if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return fail(ORION_E_NOMEM, "cudaMalloc");
+  if (cudaMallocAsync(&p, std::max<size_t>(n, 1) * sizeof(T), c->stream) != cudaSuccess)
+    return fail(ORION_E_NOMEM, "cudaMallocAsync");
   c->allocs.push_back(p);
-  CUDA_TRY(cudaMemset(p, 0, std::max<size_t>(n, 1) * sizeof(T)));
+  CUDA_TRY(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(T), c->stream));
   *dptr = static_cast<T*>(p);
   return 0;
 }
@@ -298,12 +301,12 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
       const BlockDev<float>* b32 = c->bd32.empty() ? nullptr : &c->bd32[b];
       void* dk = b64 ? (void*)b64->koff : (void*)b32->koff;
       void* dn = b64 ? (void*)b64->sk_nat : (void*)b32->sk_nat;
-      CUDA_TRY(cudaMemcpy(dk, koffs[b].data(), koffs[b].size() * 4, cudaMemcpyHostToDevice));
-      CUDA_TRY(cudaMemcpy(dn, nat.data(), nat.size() * 4, cudaMemcpyHostToDevice));
+      CUDA_TRY(cudaMemcpyAsync(dk, koffs[b].data(), koffs[b].size() * 4, cudaMemcpyHostToDevice, c->stream));
+      CUDA_TRY(cudaMemcpyAsync(dn, nat.data(), nat.size() * 4, cudaMemcpyHostToDevice, c->stream));
       std::vector<int> nbv;
       plane_major_neighbours(h, koffs[b], nat, nbv);
       void* dnb = b64 ? (void*)b64->sk_nb : (void*)b32->sk_nb;
-      CUDA_TRY(cudaMemcpy(dnb, nbv.data(), nbv.size() * 4, cudaMemcpyHostToDevice));
+      CUDA_TRY(cudaMemcpyAsync(dnb, nbv.data(), nbv.size() * 4, cudaMemcpyHostToDevice, c->stream));
     }
     // FP32 sweeps fit 512 threads per CTA without spilling, FP64 sweeps 256
     const int nt = c->prec == ORION_PREC_FP64 ? 256 : 512;
@@ -547,13 +550,45 @@ int dispatch(orion_case_t c, F fn) {
   return 0;
 }
 
+// Pinned host rings for orion_step_submit, kept for the life of the process:
+// freeing pinned memory may synchronise the device, which a request loop that
+// retires one case while others run must not do.
+static std::mutex g_ring_mu;
+
+// Case creation and destruction, graph capture and parameter changes are
+// serialised across host threads (a request loop builds cases on one thread
+// while it steps others on another); launches and copies are not.
+static std::mutex g_struct_mu;
+static std::vector<ResidualOut*> g_free_rings;
+
+static ResidualOut* acquire_hist_ring() {
+  {
+    std::lock_guard<std::mutex> lk(g_ring_mu);
+    if (!g_free_rings.empty()) {
+      ResidualOut* r = g_free_rings.back();
+      g_free_rings.pop_back();
+      return r;
+    }
+  }
+  ResidualOut* r = nullptr;
+  if (cudaMallocHost((void**)&r, sizeof(ResidualOut) * kHistCap) != cudaSuccess) return nullptr;
+  return r;
+}
+
+static void release_hist_ring(ResidualOut* r) {
+  std::lock_guard<std::mutex> lk(g_ring_mu);
+  g_free_rings.push_back(r);
+}
+
 void destroy_case(orion_case_t c) {
   if (!c) return;
   if (c->graph) cudaGraphExecDestroy(c->graph);
-  for (void* p : c->allocs) cudaFree(p);
-  if (c->arena) cudaFree(c->arena);
-  if (c->d_blocks) cudaFree(c->d_blocks);
+  // stream-ordered frees: no device-wide synchronisation while other cases run
+  for (void* p : c->allocs) cudaFreeAsync(p, c->stream);
+  if (c->arena) cudaFreeAsync(c->arena, c->stream);
+  if (c->d_blocks) cudaFreeAsync(c->d_blocks, c->stream);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  if (c->hist_host) release_hist_ring(c->hist_host);
   delete c;
 }
 
@@ -594,6 +629,7 @@ static int capture_step(orion_case_t c, cudaGraph_t* g) {
 
 static int ensure_graph(orion_case_t c) {
   if (c->graph) return 0;
+  std::lock_guard<std::mutex> lk(g_struct_mu);
   cudaGraph_t g;
   int rc = capture_step(c, &g);
   if (rc && (c->L.persist_grid > 0 || c->L.cl_size > 0)) {
@@ -674,6 +710,7 @@ size_t orion_footprint_estimate(int nblocks, const orion_block_desc_t* blocks, i
 int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion_params_t* params, int precision,
                       orion_case_t* out) {
   if (!out || !params) return fail(ORION_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(g_struct_mu);
   *out = nullptr;
   if (precision != ORION_PREC_FP64 && precision != ORION_PREC_MIXED) return fail(ORION_E_INVALID, "bad precision");
   int rc = validate_blocks(nblocks, blocks);
@@ -683,6 +720,11 @@ int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion
   c->prec = precision;
   CUDA_TRY(cudaGetDevice(&c->device));
   set_params_dev(c->P, *params);
+  // The case's own stream first: its memory is allocated and freed in stream
+  // order on it, so making or freeing a case never waits for other cases' work.
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(ORION_E_CUDA, "cudaStreamCreate");
+  c->own_stream = true;
 
   c->hb.resize(nblocks);
   long long tot = 0;
@@ -715,12 +757,12 @@ int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion
     boff[b] = total;
     total += block_bytes(c->hb[b], ssz);
   }
-  if (cudaMalloc(&c->arena, total) != cudaSuccess) {
+  if (cudaMallocAsync(&c->arena, total, c->stream) != cudaSuccess) {
     cudaGetLastError();
     return fail(ORION_E_NOMEM, "device arena of " + std::to_string(total) + " bytes");
   }
   c->arena_bytes = total;
-  CUDA_TRY(cudaMemset(c->arena, 0, total));
+  CUDA_TRY(cudaMemsetAsync(c->arena, 0, total, c->stream));
   std::vector<long long> prim_off(nblocks);
   long long ib = 0;
   if (precision == ORION_PREC_FP64) {
@@ -731,8 +773,9 @@ int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion
       ib += (long long)c->hb[b].idim * c->hb[b].jdim * c->hb[b].kdim;
       prim_off[b] = (c->bd64[b].prim - static_cast<double*>(c->arena));
     }
-    CUDA_TRY(cudaMalloc(&c->d_blocks, sizeof(BlockDev<double>) * nblocks));
-    CUDA_TRY(cudaMemcpy(c->d_blocks, c->bd64.data(), sizeof(BlockDev<double>) * nblocks, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMallocAsync(&c->d_blocks, sizeof(BlockDev<double>) * nblocks, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->d_blocks, c->bd64.data(), sizeof(BlockDev<double>) * nblocks, cudaMemcpyHostToDevice,
+                             c->stream));
   } else {
     c->bd32.resize(nblocks);
     for (int b = 0; b < nblocks; ++b) {
@@ -741,8 +784,9 @@ int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion
       ib += (long long)c->hb[b].idim * c->hb[b].jdim * c->hb[b].kdim;
       prim_off[b] = (c->bd32[b].prim - static_cast<double*>(c->arena));
     }
-    CUDA_TRY(cudaMalloc(&c->d_blocks, sizeof(BlockDev<float>) * nblocks));
-    CUDA_TRY(cudaMemcpy(c->d_blocks, c->bd32.data(), sizeof(BlockDev<float>) * nblocks, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMallocAsync(&c->d_blocks, sizeof(BlockDev<float>) * nblocks, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->d_blocks, c->bd32.data(), sizeof(BlockDev<float>) * nblocks, cudaMemcpyHostToDevice,
+                             c->stream));
   }
 
   // physical-BC dq mask (set_boundary_dq_zero windows, StateUpdater.cpp:447-468)
@@ -758,7 +802,7 @@ int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion
               mask[(size_t)i + (size_t)h.nx * ((size_t)j + (size_t)h.ny * k)] = 1;
     }
     const uint8_t* dmask = precision == ORION_PREC_FP64 ? c->bd64[b].bcmask : c->bd32[b].bcmask;
-    CUDA_TRY(cudaMemcpy((void*)dmask, mask.data(), mask.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpyAsync((void*)dmask, mask.data(), mask.size(), cudaMemcpyHostToDevice, c->stream));
   }
 
   if ((rc = build_lists(c.get(), prim_off))) {
@@ -771,10 +815,8 @@ int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion
     destroy_case(c.release());
     return rc;
   }
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
-    return fail(ORION_E_CUDA, "cudaStreamCreate");
-  c->own_stream = true;
-  CUDA_TRY(cudaDeviceSynchronize());
+  // creation-time copies and memsets are ordered on the case's stream
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
   *out = c.release();
   return 0;
 }
@@ -782,6 +824,7 @@ int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion
 int orion_case_destroy(orion_case_t c) {
   if (!c) return 0;
   cudaStreamSynchronize(c->stream);
+  std::lock_guard<std::mutex> lk(g_struct_mu);
   destroy_case(c);
   return 0;
 }
@@ -806,6 +849,7 @@ int orion_case_set_stream(orion_case_t c, void* stream) {
 
 int orion_case_set_params(orion_case_t c, const orion_params_t* params) {
   if (!c || !params) return fail(ORION_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(g_struct_mu);
   set_params_dev(c->P, *params);
   if (c->graph) {  // the captured step holds the old values: capture again on the next step
     cudaGraphExecDestroy(c->graph);
@@ -859,19 +903,23 @@ int orion_case_upload(orion_case_t c, int block, int field, const double* host) 
   if (rc) return rc;
   if (!host) return fail(ORION_E_INVALID, "null host pointer");
   const size_t n = (size_t)c->hb[block].npad * nc;
+  // Copies go on the case's own stream: a cudaMemcpy from pageable memory on
+  // the legacy stream may return before the data reach the device, and kernels
+  // on the case's (non-blocking) stream would not be ordered after it.
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   if (st && c->prec != ORION_PREC_FP64) {
     std::vector<float> tmp(n);
     for (size_t i = 0; i < n; ++i) tmp[i] = (float)host[i];
-    CUDA_TRY(cudaMemcpy(d, tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpyAsync(d, tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
   } else {
-    CUDA_TRY(cudaMemcpy(d, host, n * sizeof(double), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpyAsync(d, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   }
   if (field == ORION_FIELD_METRICS || field == ORION_FIELD_VOL) {
     rc = dispatch(c, [&](const StageOps& o) { return o.skew_static(c, block); });
     if (rc) return rc;
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
   }
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
   return 0;
 }
 
@@ -883,13 +931,14 @@ int orion_case_download(orion_case_t c, int block, int field, double* host) {
   if (rc) return rc;
   if (!host) return fail(ORION_E_INVALID, "null host pointer");
   const size_t n = (size_t)c->hb[block].npad * nc;
-  CUDA_TRY(cudaStreamSynchronize(c->stream));
   if (st && c->prec != ORION_PREC_FP64) {
     std::vector<float> tmp(n);
-    CUDA_TRY(cudaMemcpy(tmp.data(), d, n * sizeof(float), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpyAsync(tmp.data(), d, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
     for (size_t i = 0; i < n; ++i) host[i] = (double)tmp[i];
   } else {
-    CUDA_TRY(cudaMemcpy(host, d, n * sizeof(double), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpyAsync(host, d, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
   }
   return 0;
 }
@@ -945,6 +994,7 @@ int orion_residual_compute(orion_case_t c, orion_residual_t* out) {
   CUDA_TRY(cudaMemcpy(&cnt, c->L.counter, sizeof(int), cudaMemcpyDeviceToHost));
   int rc = dispatch(c, [&](const StageOps& o) { return o.residual(c); });
   if (rc) return rc;
+  c->hist_count = cnt + 1;
   return read_hist(c, cnt, 1, out);
 }
 
@@ -959,12 +1009,19 @@ int orion_phydtime(orion_case_t c, double* out) {
   return 0;
 }
 
-int orion_step_async(orion_case_t c, int nsteps) {
-  if (!c || nsteps < 0) return fail(ORION_E_INVALID, "bad arguments");
+static int launch_steps(orion_case_t c, int nsteps) {
   int rc = ensure_graph(c);
   if (rc) return rc;
   for (int s = 0; s < nsteps; ++s) CUDA_TRY(cudaGraphLaunch(c->graph, c->stream));
   c->steps_done += nsteps;
+  return 0;
+}
+
+int orion_step_async(orion_case_t c, int nsteps) {
+  if (!c || nsteps < 0) return fail(ORION_E_INVALID, "bad arguments");
+  int rc = launch_steps(c, nsteps);
+  if (rc) return rc;
+  if (c->hist_count >= 0) c->hist_count += nsteps;
   return 0;
 }
 
@@ -976,14 +1033,15 @@ int orion_step(orion_case_t c, int nsteps, orion_residual_t* hist) {
   int done = 0;
   while (done < nsteps) {
     const int n = std::min(nsteps - done, kHistCap);
-    int rc = orion_step_async(c, n);
+    int rc = launch_steps(c, n);
     if (rc) return rc;
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (c->L.sweep_ctl) {
       int ctl[2] = {0, 0};
       CUDA_TRY(cudaMemcpy(ctl, c->L.sweep_ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
       if (ctl[1]) {
-        CUDA_TRY(cudaMemset(c->L.sweep_ctl, 0, sizeof(ctl)));
+        CUDA_TRY(cudaMemsetAsync(c->L.sweep_ctl, 0, sizeof(ctl), c->stream));
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
         return fail(ORION_E_TIMEOUT, "a grid barrier of the implicit sweeps gave up waiting");
       }
     }
@@ -993,8 +1051,80 @@ int orion_step(orion_case_t c, int nsteps, orion_residual_t* hist) {
     }
     done += n;
   }
+  c->hist_count = (long long)cnt + nsteps;
   CUDA_TRY(cudaGetLastError());
   return 0;
+}
+
+// Reads the sweep barrier's error flag (the stream is idle).
+static int sweep_status(orion_case_t c) {
+  if (!c->L.sweep_ctl) return 0;
+  int ctl[2] = {0, 0};
+  CUDA_TRY(cudaMemcpy(ctl, c->L.sweep_ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
+  if (ctl[1]) {
+    CUDA_TRY(cudaMemsetAsync(c->L.sweep_ctl, 0, sizeof(ctl), c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return fail(ORION_E_TIMEOUT, "a grid barrier of the implicit sweeps gave up waiting");
+  }
+  return 0;
+}
+
+int orion_step_submit(orion_case_t c, int nsteps) {
+  if (!c || nsteps < 0) return fail(ORION_E_INVALID, "bad arguments");
+  if (c->pending_n + nsteps > kHistCap)
+    return fail(ORION_E_INVALID, "more unpolled steps than the history ring holds (4096)");
+  if (!c->hist_host && !(c->hist_host = acquire_hist_ring()))
+    return fail(ORION_E_NOMEM, "pinned history ring");
+  if (c->hist_count < 0) {  // once: learn the device counter
+    int cnt = 0;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    CUDA_TRY(cudaMemcpy(&cnt, c->L.counter, sizeof(int), cudaMemcpyDeviceToHost));
+    c->hist_count = cnt;
+  }
+  if (nsteps == 0) return 0;
+  int rc = launch_steps(c, nsteps);
+  if (rc) return rc;
+  // the new entries sit at ring positions [first, first + nsteps) mod kHistCap
+  const long long first = c->hist_count;
+  long long pos = first % kHistCap;
+  int left = nsteps;
+  while (left > 0) {
+    const int n = (int)std::min<long long>(left, kHistCap - pos);
+    CUDA_TRY(cudaMemcpyAsync(c->hist_host + pos, c->L.hist + pos, sizeof(ResidualOut) * n, cudaMemcpyDeviceToHost,
+                             c->stream));
+    left -= n;
+    pos = 0;
+  }
+  if (c->pending_n == 0) c->pending_first = first;
+  c->pending_n += nsteps;
+  c->hist_count += nsteps;
+  return 0;
+}
+
+int orion_case_poll(orion_case_t c, orion_residual_t* out, int cap, int* n) {
+  if (!c || !n || (cap > 0 && !out)) return fail(ORION_E_INVALID, "null argument");
+  *n = 0;
+  const cudaError_t q = cudaStreamQuery(c->stream);
+  if (q == cudaErrorNotReady) return 0;
+  if (q != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ORION_E_CUDA, std::string("case stream: ") + cudaGetErrorString(q));
+  }
+  int rc = sweep_status(c);
+  if (rc) return rc;
+  const int take = std::min(cap, c->pending_n);
+  for (int s = 0; s < take; ++s) {
+    const ResidualOut& r = c->hist_host[(c->pending_first + s) % kHistCap];
+    out[s].rms = r.rms;
+    out[s].max = r.max;
+    for (int m = 0; m < 5; ++m) out[s].max_loc[m] = r.loc[m];
+    out[s].pad = 0;
+    out[s].phydtime = r.phydtime;
+  }
+  c->pending_first += take;
+  c->pending_n -= take;
+  *n = take;
+  return 1;
 }
 
 int orion_last_residual(orion_case_t c, orion_residual_t* out) {

@@ -1,3 +1,4 @@
+#include <mutex>
 // Stage launchers, templated on storage S and compute T.  Included by exactly
 // one translation unit per precision.
 #pragma once
@@ -16,8 +17,15 @@ struct Stages {
   static const BlockDev<S>* blocks(orion_case_t c) { return static_cast<const BlockDev<S>*>(c->d_blocks); }
 
   // Line kernels take up to kLineSmemBudget of dynamic shared memory; the
-  // attribute is set once, before any stream capture.
+  // attribute is set once per process, before any stream capture.
   static int set_attributes() {
+    static std::once_flag once;
+    static int rc = 0;
+    std::call_once(once, [] { rc = set_line_attributes(); });
+    return rc;
+  }
+
+  static int set_line_attributes() {
     const int b = (int)kLineSmemBudget;
     CUDA_TRY(cudaFuncSetAttribute(k_viscous<0, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
     CUDA_TRY(cudaFuncSetAttribute(k_viscous<1, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
@@ -131,20 +139,32 @@ struct Stages {
     return sizeof(SweepBlock<S>) * c->nblocks + sizeof(SweepSlot) * 2 * (size_t)c->L.max_planes;
   }
 
+  // The cluster kernel's function attributes are process-wide: they are set
+  // once, to the largest shared memory any case may ask for, and never per
+  // case (a case made on one host thread must not change an attribute that a
+  // graph of another case, captured on another thread, was built against).
+  static constexpr size_t kClusterSmemMax = 200 * 1024;
+
+  template <int NT>
+  static bool cluster_attributes() {
+    static std::once_flag once;
+    static bool ok = false;
+    std::call_once(once, [] {
+      auto kern = k_sweeps_cluster<S, T, NT>;
+      ok = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClusterSmemMax) ==
+               cudaSuccess &&
+           cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
+      if (!ok) cudaGetLastError();
+    });
+    return ok;
+  }
+
   template <int NT>
   static int cluster_setup(orion_case_t c) {
     auto kern = k_sweeps_cluster<S, T, NT>;
     const size_t smem = cluster_smem(c);
-    if (smem > 200 * 1024) return 0;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
-      cudaGetLastError();
-      return 0;
-    }
+    if (smem > kClusterSmemMax || !cluster_attributes<NT>()) return 0;
     for (int cs : {16, 8}) {
-      if (cs > 8 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
-        cudaGetLastError();
-        continue;
-      }
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3(cs * 64);
       cfg.blockDim = dim3(NT);

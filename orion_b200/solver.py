@@ -197,6 +197,28 @@ class FlowFieldSet:
     def step_async(self, nsteps: int):
         check(_lib.load().orion_step_async(self._h, nsteps))
 
+    def submit(self, nsteps: int):
+        """Enqueues nsteps steps and the asynchronous copy of their residual
+        history; returns at once (orion_step_submit)."""
+        check(_lib.load().orion_step_submit(self._h, nsteps))
+
+    def poll(self, cap: int = 4096):
+        """None while submitted steps run; else their history (n, 8) as step() returns it."""
+        buf = (_lib.Residual * max(cap, 1))()
+        n = C.c_int()
+        rc = _lib.load().orion_case_poll(self._h, buf, cap, C.byref(n))
+        if rc == 0:
+            return None
+        check(rc if rc < 0 else 0)
+        out = np.zeros((n.value, 8))
+        for s in range(n.value):
+            r = buf[s]
+            out[s, 0] = r.rms
+            out[s, 1] = r.max
+            out[s, 2:7] = list(r.max_loc)
+            out[s, 7] = r.phydtime
+        return out
+
     def last_residual(self) -> ResidualStats:
         r = _lib.Residual()
         check(_lib.load().orion_last_residual(self._h, C.byref(r)))

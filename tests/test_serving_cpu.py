@@ -1,0 +1,120 @@
+"""Host logic of the request loop (orion_b200.serving) with fake device cases.
+
+The fake case runs `submit`ted steps instantly and reports a residual history
+rms_k = r0 * decay**(k-1) (NaN from step `nan_at` on).  Checks: admission
+never exceeds the HBM budget, requests are admitted first come first served,
+a case retires at the end of the quantum in which its residual dropped to
+`drop` x its first-step residual, at max_steps, or when it stops being
+finite, and a request larger than the whole budget is rejected.
+"""
+import math
+
+import numpy as np
+
+from orion_b200 import serving
+
+
+class FakeCase:
+    def __init__(self, req, log):
+        self.req = req
+        self.log = log
+        self.k = 0
+        self.pending = 0
+        self.closed = False
+
+    def submit(self, n):
+        self.pending += n
+
+    def poll(self, cap=4096):
+        if not self.pending:
+            return None
+        rows = []
+        for _ in range(self.pending):
+            self.k += 1
+            r = self.req.decay ** (self.k - 1) if self.k < self.req.nan_at else math.nan
+            rows.append([r, r, 0, 1, 1, 1, 1, 0.0])
+        self.pending = 0
+        return np.array(rows)
+
+    def close(self):
+        self.closed = True
+        self.log.append(("close", self.req.rid))
+
+
+class FakeServer(serving.Server):
+    def __init__(self, sizes, **kw):
+        self.sizes = sizes
+        self.log = []
+        self.resident = 0
+        self.max_resident_bytes = 0
+        super().__init__(hbm_budget=kw.pop("hbm_budget"), clock=self._clock, **kw)
+        self.t = 0.0
+
+    def _clock(self):
+        self.t = getattr(self, "t", 0.0) + 0.001  # 1 ms per look at the clock
+        return self.t
+
+    def footprint(self, req):
+        return self.sizes[req.rid]
+
+    def make_case(self, req):
+        self.log.append(("admit", req.rid))
+        return FakeCase(req, self.log)
+
+
+def _req(rid, arrival, decay=0.5, nan_at=10 ** 9, max_steps=100):
+    r = serving.Request(rid=rid, arrival_s=arrival, dims=(33, 33, 33), nblocks=1, height=0.05, moo=0.5,
+                        reynolds=1e3, noise_seed=rid, max_steps=max_steps, drop=1e-3)
+    r.decay, r.nan_at = decay, nan_at
+    return r
+
+
+def test_retirement_rules_and_quanta():
+    reqs = [_req(0, 0.0, decay=0.5),                 # 0.5**10 < 1e-3 at step 11
+            _req(1, 0.0, decay=0.99, max_steps=30),  # never drops: stops at max_steps
+            _req(2, 0.0, decay=0.9, nan_at=7)]       # NaN at step 7
+    srv = FakeServer({0: 10, 1: 10, 2: 10}, hbm_budget=100, quantum=5)
+    res = {r.rid: r for r in srv.run(reqs)}
+    assert res[0].status == "converged" and res[0].steps_to_drop == 11 and res[0].steps == 15
+    assert res[1].status == "max_steps" and res[1].steps == 30
+    assert res[2].status == "diverged" and res[2].steps == 10
+    assert all(r.latency_s > 0 for r in res.values())
+
+
+def test_admission_respects_hbm_budget_and_arrival_order():
+    sizes = {0: 60, 1: 50, 2: 30, 3: 40}
+    reqs = [_req(i, 0.001 * i, decay=0.5) for i in range(4)]
+    srv = FakeServer(sizes, hbm_budget=100, quantum=4)
+    res = srv.run(reqs)
+    assert [r.status for r in res] == ["converged"] * 4
+    admits = [rid for ev, rid in srv.log if ev == "admit"]
+    assert admits == [0, 1, 2, 3]  # first come, first served
+    # replay the log: resident bytes never above the budget
+    used, peak = 0, 0
+    for ev, rid in srv.log:
+        used += sizes[rid] if ev == "admit" else -sizes[rid]
+        peak = max(peak, used)
+    assert peak <= 100
+    assert srv.peak_bytes <= 100
+
+
+def test_request_larger_than_budget_is_rejected():
+    srv = FakeServer({0: 500, 1: 10}, hbm_budget=100, quantum=4)
+    res = {r.rid: r for r in srv.run([_req(0, 0.0), _req(1, 0.0)])}
+    assert res[0].status == "rejected"
+    assert res[1].status == "converged"
+
+
+def test_c4_request_stream_is_seeded_and_within_ranges():
+    a = serving.c4_requests(64, seed=4)
+    b = serving.c4_requests(64, seed=4)
+    assert [(r.dims, r.arrival_s, r.moo) for r in a] == [(r.dims, r.arrival_s, r.moo) for r in b]
+    gaps = np.diff([0.0] + [r.arrival_s for r in a])
+    assert 0.02 < gaps.mean() < 0.1  # mean inter-arrival 50 ms
+    for r in a:
+        assert set(r.dims) <= set(serving.DIMS)
+        assert 1 <= r.nblocks <= 8 and 0.2 <= r.moo <= 0.85 and 1e3 <= r.reynolds <= 1e5
+        assert 0.02 <= r.height <= 0.08
+        split = r.split()
+        assert sorted(split)[:2] == [1, 1]  # one split axis at most
+        assert serving._footprint_dims(r, 1) > 0
