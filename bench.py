@@ -206,7 +206,6 @@ def main():
     rep = replicas.from_env()
     K, W = args.steps, args.warmup
     npts = case.npoints
-    metrics = [solver.grid_metrics(b, case.params.gcl) for b in case.blocks]
     barrier, max_over_ranks = rep.barrier, rep.max_over_ranks
 
     def timed_steps(fs, nsteps):
@@ -225,7 +224,7 @@ def main():
     results = {}
     states = {}
     for name, prec in (("mixed", _lib.PREC_MIXED), ("plain", _lib.PREC_FP64)):
-        fs = solver.FlowFieldSet(case, precision=prec, device=local, metrics=metrics)
+        fs = solver.FlowFieldSet(case, precision=prec, device=local)
         fs.step(L2_STEPS)
         states[name] = [fs.download(b, "prim")[:5, 3:-3, 3:-3, 3:-3] for b in range(len(case.blocks))]
         fs.step(W)

@@ -147,6 +147,13 @@ int orion_case_download(orion_case_t c, int block, int field, double* host);
  * 2n+1 and 2n+2 scale rho and u at padded point n (blocks in order, k,j,i). */
 int orion_case_init_flow(orion_case_t c, uint64_t seed, double amp);
 
+/* Grid metrics and Jacobian of one block computed on the device into the
+ * case's METRICS and VOL fields (compute_grid_metrics + check_grid_metrics,
+ * src/mesh/MetricComputer.cpp:103-500): x,y,z are the block's host
+ * coordinates, idim*jdim*kdim, i fastest (Plot3D order).  Bit-identical to
+ * orion_grid_metrics_host; gcl=1 selects the Visbal conservative form.  Waits. */
+int orion_case_grid_metrics(orion_case_t c, int block, const double* x, const double* y, const double* z, int gcl);
+
 /* Grid metrics and Jacobian of one block on the host (compute_grid_metrics +
  * check_grid_metrics, src/mesh/MetricComputer.cpp:103-500): x,y,z are
  * idim*jdim*kdim, i fastest; metrics (9 comps) and vol are written in the

@@ -50,6 +50,7 @@ SIGNATURES = {
     "orion_case_destroy": (C.c_int, [C.c_void_p]),
     "orion_case_set_params": (C.c_int, [C.c_void_p, C.POINTER(Params)]),
     "orion_step_submit": (C.c_int, [C.c_void_p, C.c_int]),
+    "orion_case_grid_metrics": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "orion_case_poll": (C.c_int, [C.c_void_p, C.POINTER(Residual), C.c_int, C.POINTER(C.c_int)]),
     "orion_case_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "orion_case_sync": (C.c_int, [C.c_void_p]),

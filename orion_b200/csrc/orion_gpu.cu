@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "case.hpp"
+#include "metrics_dev.cuh"
 
 using namespace orion;
 
@@ -940,6 +941,45 @@ int orion_case_download(orion_case_t c, int block, int field, double* host) {
     CUDA_TRY(cudaMemcpyAsync(host, d, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
   }
+  return 0;
+}
+
+int orion_case_grid_metrics(orion_case_t c, int block, const double* x, const double* y, const double* z, int gcl) {
+  if (!c || block < 0 || block >= c->nblocks || !x || !y || !z) return fail(ORION_E_INVALID, "bad arguments");
+  const auto& h = c->hb[block];
+  const long long n = (long long)h.idim * h.jdim * h.kdim;
+  void* dmet;
+  void* dvol;
+  int nc;
+  bool st;
+  int rc = field_info(c, block, ORION_FIELD_METRICS, &dmet, &nc, &st);
+  if (!rc) rc = field_info(c, block, ORION_FIELD_VOL, &dvol, &nc, &st);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  double* dxyz = nullptr;
+  double* dD = nullptr;
+  if (cudaMallocAsync((void**)&dxyz, sizeof(double) * 3 * n, c->stream) != cudaSuccess ||
+      cudaMallocAsync((void**)&dD, sizeof(double) * 9 * n, c->stream) != cudaSuccess) {
+    cudaGetLastError();
+    if (dxyz) cudaFreeAsync(dxyz, c->stream);
+    return fail(ORION_E_NOMEM, "grid metrics scratch");
+  }
+  CUDA_TRY(cudaMemcpyAsync(dxyz, x, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(dxyz + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(dxyz + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(cudaMemsetAsync(dmet, 0, sizeof(double) * 9 * (size_t)h.npad, c->stream));  // ghosts stay zero
+  CUDA_TRY(cudaMemsetAsync(dvol, 0, sizeof(double) * (size_t)h.npad, c->stream));
+  const gm::GridDims G{h.idim, h.jdim, h.kdim, n};
+  const int nblk = (int)((n + kThreads - 1) / kThreads);
+  gm::k_coord_derivs<<<nblk, kThreads, 0, c->stream>>>(G, dxyz, dD);
+  gm::k_metrics_final<<<nblk, kThreads, 0, c->stream>>>(G, h.nx, h.ny, h.npad, gcl, dxyz, dD,
+                                                       static_cast<double*>(dmet), static_cast<double*>(dvol));
+  CUDA_TRY(cudaGetLastError());
+  cudaFreeAsync(dxyz, c->stream);
+  cudaFreeAsync(dD, c->stream);
+  rc = dispatch(c, [&](const StageOps& o) { return o.skew_static(c, block); });
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
   return 0;
 }
 

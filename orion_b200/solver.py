@@ -104,11 +104,15 @@ class FlowFieldSet:
                                     C.byref(h)))
         self._h = h
         self._keep = keep
-        if metrics is None:
-            metrics = [grid_metrics(b, case.params.gcl) for b in case.blocks]
-        for n, (met, vol) in enumerate(metrics):
-            self.upload(n, "metrics", met)
-            self.upload(n, "vol", vol)
+        if metrics is None:  # on the device, from the coordinates
+            for n, b in enumerate(case.blocks):
+                x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (b.x, b.y, b.z))
+                check(lib.orion_case_grid_metrics(self._h, n, x.ctypes.data, y.ctypes.data, z.ctypes.data,
+                                                  case.params.gcl))
+        else:
+            for n, (met, vol) in enumerate(metrics):
+                self.upload(n, "metrics", met)
+                self.upload(n, "vol", vol)
         if init:
             check(lib.orion_case_init_flow(self._h, case.noise_seed, case.noise_amp))
             self.sync()
