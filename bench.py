@@ -176,6 +176,9 @@ def main():
     ap.add_argument("--config", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=24,
+                    help="requests of the bounded serving run (0: skip it)")
+    ap.add_argument("--serve-max-steps", type=int, default=200)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -203,10 +206,10 @@ def main():
 
     import torch
     from orion_b200 import _lib, replicas, solver
-    rep = replicas.from_env()
+    group = replicas.from_env()
     K, W = args.steps, args.warmup
     npts = case.npoints
-    barrier, max_over_ranks = rep.barrier, rep.max_over_ranks
+    barrier, max_over_ranks = group.barrier, group.max_over_ranks
 
     def timed_steps(fs, nsteps):
         s = torch.cuda.ExternalStream(fs.stream_ptr())
@@ -240,8 +243,8 @@ def main():
     l2 = (num / den) ** 0.5
     per_rank_pts = npts * K
     mixed_ms, plain_ms = results["mixed"]["ms"], results["plain"]["ms"]
-    value = rep.aggregate_rate(per_rank_pts, mixed_ms / 1e3)
-    plain_value = rep.aggregate_rate(per_rank_pts, plain_ms / 1e3)
+    value = group.aggregate_rate(per_rank_pts, mixed_ms / 1e3)
+    plain_value = group.aggregate_rate(per_rank_pts, plain_ms / 1e3)
 
     # per-stage timing of one step on the mixed case -> dominant stage roofline
     fsm = results["mixed"]["fs"]
@@ -308,7 +311,27 @@ def main():
             _lib.check(lib.orion_case_download(fse.handle, b, _lib.FIELD_PRIM, C.c_void_p(t.data_ptr())))
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = rep.aggregate_rate(npts * ne, e2e_s)
+    e2e_value = group.aggregate_rate(npts * ne, e2e_s)
+
+    # bounded serving run: seeded request stream (Poisson arrivals, mixed sizes and
+    # flow conditions), continuous batching on the mixed path against the same
+    # requests served one at a time on the plain FP64 path
+    ws_gb = fsm.footprint() / 1e9
+    serving_out = None
+    if args.serve_requests > 0:
+        from orion_b200 import serving
+        for r in results.values():
+            r["fs"].close()
+        reqs = serving.c4_requests(args.serve_requests, seed=4, mean_ms=50.0, max_steps=args.serve_max_steps)
+        srv = serving.Server(_lib.PREC_MIXED, device=local, quantum=20)
+        mixed_s = serving.summarize(srv.run(reqs))
+        mixed_s["peak_resident_cases"] = srv.peak_resident
+        seq = serving.Server(_lib.PREC_FP64, device=local, quantum=20, max_active=1)
+        plain_s = serving.summarize(seq.run(reqs))
+        serving_out = {"requests": args.serve_requests, "max_steps": args.serve_max_steps, "drop": 1e-6,
+                       "mean_interarrival_ms": 50.0,
+                       "mixed_continuous": mixed_s, "plain_one_at_a_time": plain_s,
+                       "throughput_ratio": mixed_s["cell_updates_per_s"] / plain_s["cell_updates_per_s"]}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -325,7 +348,7 @@ def main():
             "config": {"workload": case.name + " mixed-batched", "points": npts, "blocks": len(case.blocks),
                        "mach": case.params.moo, "reynolds": case.params.reynolds,
                        "l2_flush": "none needed: working set %.1f GB per GPU > 126 MB L2" %
-                                   (fsm.footprint() / 1e9)},
+                                   ws_gb},
             "plain_fp64": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_ms / K, "dtype": "f64"},
             "mixed_over_plain": plain_ms / mixed_ms,
             "sweep_schedule": {"mixed": results["mixed"]["sweeps"], "plain": results["plain"]["sweeps"]},
@@ -335,13 +358,14 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": ne},
+            "serving": serving_out,
             "gpu_launches": results["mixed"]["launches"] * K,
             "clocks": clk,
         }
         print(json.dumps(line))
     for r in results.values():
         r["fs"].close()
-    rep.close()
+    group.close()
 
 
 if __name__ == "__main__":

@@ -355,11 +355,14 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
         queue.push_back(std::move(msg));
       }
     }
-    std::map<long long, long long> dst2src;  // last writer wins
-    std::vector<long long> order;
+    // last writer wins; destinations in order of first appearance.  Dense per
+    // block (slot of each padded prim element), so building it is O(points).
+    std::vector<long long> hs, hd;
+    std::vector<int> slot;
     for (int b = 0; b < nb; ++b) {
       const auto& h = c->hb[b];
       const int dims[3] = {h.idim, h.jdim, h.kdim};
+      slot.assign((size_t)5 * h.npad, -1);
       for (int r = 0; r < (int)h.regions.size(); ++r) {
         const auto& hr = h.regions[r];
         if (hr.r.nbt <= 0) continue;
@@ -375,17 +378,18 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
             for (int i = beg[0]; i <= end[0]; ++i) pts.push_back(i + (long long)h.nx * (j + (long long)h.ny * k));
         const size_t np = pts.size();
         for (size_t q = 0; q < 5 * np && q < it->src.size(); ++q) {
-          const long long dst = prim_off[b] + (long long)(q / np) * h.npad + pts[q % np];
-          if (!dst2src.count(dst)) order.push_back(dst);
-          dst2src[dst] = it->src[q];
+          const long long local = (long long)(q / np) * h.npad + pts[q % np];
+          int& sl = slot[(size_t)local];
+          if (sl < 0) {
+            sl = (int)hd.size();
+            hd.push_back(prim_off[b] + local);
+            hs.push_back(it->src[q]);
+          } else {
+            hs[(size_t)sl] = it->src[q];
+          }
         }
         queue.erase(it);
       }
-    }
-    std::vector<long long> hs, hd;
-    for (long long d : order) {
-      hd.push_back(d);
-      hs.push_back(dst2src[d]);
     }
     if ((rc = dev_upload(c, &L.halo_src, hs))) return rc;
     if ((rc = dev_upload(c, &L.halo_dst, hd))) return rc;
@@ -468,10 +472,16 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
         qsrc[{g.nbt - 1, g.ibcwin - 1}] = s;
       }
     }
-    std::map<std::pair<int, long long>, std::vector<int>> entries;
-    std::vector<std::pair<int, long long>> dorder;
+    // one entry per destination point, partners in region order; dense per block
+    std::vector<int> apb, apo{0}, aps;
+    std::vector<long long> api;
+    std::vector<int> eid;
+    std::vector<std::vector<int>> eslots;
     for (int b = 0; b < nb; ++b) {
       const auto& h = c->hb[b];
+      eid.assign((size_t)h.npad, -1);
+      eslots.clear();
+      std::vector<long long> eidx;
       for (int r = 0; r < (int)h.regions.size(); ++r) {
         const auto& hr = h.regions[r];
         const auto& g = hr.r;
@@ -500,20 +510,21 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
                 return fail(ORION_E_UNSUPPORTED, "interface averaging map leaves the partner window");
               const long long idx = (slo[0] + i - 1 + NG) +
                                     (long long)h.nx * ((slo[1] + j - 1 + NG) + (long long)h.ny * (slo[2] + k - 1 + NG));
-              auto key = std::make_pair(b, idx);
-              auto& e = entries[key];
-              if (e.empty()) dorder.push_back(key);
-              e.push_back(it->second.slot_base + (int)rem);
+              int& e = eid[(size_t)idx];
+              if (e < 0) {
+                e = (int)eslots.size();
+                eslots.emplace_back();
+                eidx.push_back(idx);
+              }
+              eslots[(size_t)e].push_back(it->second.slot_base + (int)rem);
             }
       }
-    }
-    std::vector<int> apb, apo{0}, aps;
-    std::vector<long long> api;
-    for (auto& key : dorder) {
-      apb.push_back(key.first);
-      api.push_back(key.second);
-      for (int s : entries[key]) aps.push_back(s);
-      apo.push_back((int)aps.size());
+      for (size_t e = 0; e < eslots.size(); ++e) {
+        apb.push_back(b);
+        api.push_back(eidx[e]);
+        for (int sl : eslots[e]) aps.push_back(sl);
+        apo.push_back((int)aps.size());
+      }
     }
     if ((rc = dev_upload(c, &L.pk_block, pkb))) return rc;
     if ((rc = dev_upload(c, &L.pk_idx, pki))) return rc;
