@@ -230,11 +230,13 @@ def main():
         fs = solver.FlowFieldSet(case, precision=prec, device=local)
         fs.step(L2_STEPS)
         states[name] = [fs.download(b, "prim")[:5, 3:-3, 3:-3, 3:-3] for b in range(len(case.blocks))]
+        tune = fs.autotune(steps_per_trial=3)  # schedule chosen by timing on this case; solution unchanged
         fs.step(W)
         if name == "mixed":
             clocks.start()
         ms = timed_steps(fs, K)
-        results[name] = {"ms": ms, "launches": fs.step_launches(), "fs": fs, "sweeps": fs.sweep_schedule()}
+        results[name] = {"ms": ms, "launches": fs.step_launches(), "fs": fs, "sweeps": fs.sweep_schedule(),
+                         "tune": tune}
         if name == "plain":
             clk = clocks.stop()
     # L2 error of the mixed state against the plain FP64 state after L2_STEPS steps
@@ -352,6 +354,7 @@ def main():
             "plain_fp64": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_ms / K, "dtype": "f64"},
             "mixed_over_plain": plain_ms / mixed_ms,
             "sweep_schedule": {"mixed": results["mixed"]["sweeps"], "plain": results["plain"]["sweeps"]},
+            "autotune": {"mixed": results["mixed"]["tune"], "plain": results["plain"]["tune"]},
             "mixed_vs_plain_rel_l2": l2, "mixed_vs_plain_l2_after_steps": L2_STEPS,
             "roofline": roofline, "step_roofline": step_roofline,
             "stage_ms": stage_ms,

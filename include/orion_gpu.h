@@ -39,6 +39,12 @@ extern "C" {
 #define ORION_PREC_FP64 0      /* plain form: every stage in FP64 */
 #define ORION_PREC_MIXED 1     /* FP32 flux/viscous/LU-SGS increments; FP64 metrics, Q update, norms */
 
+/* Forms of the LU-SGS / GS hyperplane sweeps (all give the reference's
+ * Gauss-Seidel order; they differ in how hyperplanes are separated). */
+#define ORION_SWEEP_PLANES 0   /* one launch per hyperplane */
+#define ORION_SWEEP_GRID 1     /* one cooperative launch, bounded grid barrier per hyperplane */
+#define ORION_SWEEP_CLUSTER 2  /* thread-block clusters (8 or 16 CTAs), cluster barrier per hyperplane */
+
 /* BC types (src/bc/PhysicalBC.cpp:576-613) */
 #define ORION_BC_INTERFACE (-1)
 #define ORION_BC_WALL 2
@@ -101,6 +107,16 @@ typedef struct {
 } orion_residual_t;
 
 typedef struct orion_case_s* orion_case_t;
+
+/* A step schedule: sweep form, cluster size (CLUSTER form: 8 or 16; 0 = the
+ * largest co-resident) and the grid lines per CTA of the viscous and inviscid
+ * line kernels (1-32).  ms_per_step is filled by orion_case_autotune. */
+typedef struct {
+  int sweep_form;
+  int cluster_size;
+  int lanes;
+  float ms_per_step;
+} orion_schedule_t;
 
 const char* orion_last_error(void);
 int orion_abi_version(void);
@@ -183,6 +199,21 @@ int orion_step(orion_case_t c, int nsteps, orion_residual_t* hist);
 int orion_step_async(orion_case_t c, int nsteps);
 /* Copies the residual of the most recent step (waits). */
 int orion_last_residual(orion_case_t c, orion_residual_t* out);
+
+/* Applies a schedule (deterministic: use it to fix a tuned choice).  Results
+ * do not depend on the lanes; on the plain path they do not depend on the
+ * sweep form either (the same operations in the same order). */
+int orion_case_set_schedule(orion_case_t c, const orion_schedule_t* s);
+int orion_case_get_schedule(orion_case_t c, orion_schedule_t* s);
+/* Autotuner: times candidate schedules on this case (line lanes 8/16/32 with
+ * the current sweep form, then every sweep form the device supports with the
+ * best lanes), steps_per_trial timed steps each after one warm-up step, and
+ * applies the fastest.  The state (prim, the step counter) is saved before and
+ * restored after every trial, so tuning leaves the solution where it was; the
+ * next whole step recomputes every derived field.  Fills trials[0..*ntrials)
+ * (cap entries at most) and *best.  Waits; no steps may be pending. */
+int orion_case_autotune(orion_case_t c, int steps_per_trial, orion_schedule_t* trials, int cap, int* ntrials,
+                        orion_schedule_t* best);
 
 /* Non-blocking stepping for request loops that keep many cases in flight.
  * orion_step_submit enqueues nsteps whole steps on the case's stream and an

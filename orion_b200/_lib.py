@@ -12,6 +12,8 @@ LIB_PATH = os.environ.get("ORION_GPU_LIB") or os.path.join(HERE, "liborion_gpu.s
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+SWEEP_PLANES, SWEEP_GRID, SWEEP_CLUSTER = 0, 1, 2
+SWEEP_NAMES = {SWEEP_PLANES: "planes", SWEEP_GRID: "grid", SWEEP_CLUSTER: "cluster"}
 
 FIELD_PRIM, FIELD_Q, FIELD_DQ, FIELD_METRICS, FIELD_VOL, FIELD_DT, FIELD_C, FIELD_MU = range(8)
 FIELD_NCOMP = {FIELD_PRIM: 6, FIELD_Q: 5, FIELD_DQ: 5, FIELD_METRICS: 9, FIELD_VOL: 1, FIELD_DT: 1,
@@ -36,6 +38,10 @@ class BlockDesc(C.Structure):
                 ("regions", C.POINTER(Region))]
 
 
+class Schedule(C.Structure):
+    _fields_ = [("sweep_form", C.c_int), ("cluster_size", C.c_int), ("lanes", C.c_int), ("ms_per_step", C.c_float)]
+
+
 class Residual(C.Structure):
     _fields_ = [("rms", C.c_double), ("max", C.c_double), ("max_loc", C.c_int * 5), ("pad", C.c_int),
                 ("phydtime", C.c_double)]
@@ -50,6 +56,10 @@ SIGNATURES = {
     "orion_case_destroy": (C.c_int, [C.c_void_p]),
     "orion_case_set_params": (C.c_int, [C.c_void_p, C.POINTER(Params)]),
     "orion_step_submit": (C.c_int, [C.c_void_p, C.c_int]),
+    "orion_case_set_schedule": (C.c_int, [C.c_void_p, C.POINTER(Schedule)]),
+    "orion_case_get_schedule": (C.c_int, [C.c_void_p, C.POINTER(Schedule)]),
+    "orion_case_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Schedule), C.c_int, C.POINTER(C.c_int),
+                                      C.POINTER(Schedule)]),
     "orion_case_grid_metrics": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "orion_case_poll": (C.c_int, [C.c_void_p, C.POINTER(Residual), C.c_int, C.POINTER(C.c_int)]),
     "orion_case_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),

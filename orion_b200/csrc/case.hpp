@@ -43,6 +43,7 @@ struct DeviceLists {
   LineTile* tiles[3] = {nullptr, nullptr, nullptr};
   int n_tiles[3] = {0, 0, 0};
   int lanes[3] = {1, 1, 1};
+  int lanes_cap = 32;                            // line tiles: at most this many grid lines per CTA
   int lmax[3] = {0, 0, 0};
   Chunk* sweep_chunks[2] = {nullptr, nullptr};  // forward / backward hyperplane launches
   std::vector<int> sweep_off[2];                 // host: chunk range of each launch
@@ -130,6 +131,7 @@ struct StageOps {
   int (*init_flow)(orion_case_t, uint64_t seed, double amp);
   int (*skew_static)(orion_case_t, int block);
   int (*persistent_grid)(orion_case_t);
+  int (*schedule)(orion_case_t, int form, int cluster_size);
 };
 
 // Groups the mesh blocks into `nclusters` clusters (largest first onto the

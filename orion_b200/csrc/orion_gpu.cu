@@ -246,6 +246,33 @@ namespace {
 // --------------------------------------------------------------------------
 // work-list builders
 // --------------------------------------------------------------------------
+// Line tiles per direction: up to L.lanes_cap grid lines per CTA, fewer where
+// the face fluxes of the longest line would not fit the shared-memory budget.
+int build_line_tiles(orion_case_t c) {
+  auto& L = c->L;
+  const int nb = c->nblocks;
+  const size_t tsz = (c->prec == ORION_PREC_FP64) ? 8 : 4;
+  int rc;
+  for (int d = 0; d < 3; ++d) {
+    int lmax = 0;
+    for (auto& h : c->hb) lmax = std::max(lmax, d == 0 ? h.idim : (d == 1 ? h.jdim : h.kdim));
+    L.lmax[d] = lmax;
+    int lanes = (int)std::min<size_t>((size_t)L.lanes_cap, kLineSmemBudget / ((size_t)(lmax + 1) * 5 * tsz));
+    if (lanes < 1) return fail(ORION_E_UNSUPPORTED, "grid line too long for the line kernels");
+    if (d > 0 && lanes >= 8) lanes = lanes / 8 * 8;
+    L.lanes[d] = lanes;
+    std::vector<LineTile> tiles;
+    for (int b = 0; b < nb; ++b) {
+      const auto& h = c->hb[b];
+      const int nlines = d == 0 ? h.jdim * h.kdim : (d == 1 ? h.idim * h.kdim : h.idim * h.jdim);
+      for (int s = 0; s < nlines; s += lanes) tiles.push_back(LineTile{b, s, std::min(lanes, nlines - s), 0});
+    }
+    if ((rc = dev_upload(c, &L.tiles[d], tiles))) return rc;
+    L.n_tiles[d] = (int)tiles.size();
+  }
+  return 0;
+}
+
 int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
   auto& L = c->L;
   const int nb = c->nblocks;
@@ -268,25 +295,7 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
   L.n_int_chunks = (int)itr.size();
   if ((rc = dev_upload(c, &L.pad_base, pad_base))) return rc;
 
-  // line tiles per direction
-  const size_t tsz = (c->prec == ORION_PREC_FP64) ? 8 : 4;
-  for (int d = 0; d < 3; ++d) {
-    int lmax = 0;
-    for (auto& h : c->hb) lmax = std::max(lmax, d == 0 ? h.idim : (d == 1 ? h.jdim : h.kdim));
-    L.lmax[d] = lmax;
-    int lanes = (int)std::min<size_t>(32, kLineSmemBudget / ((size_t)(lmax + 1) * 5 * tsz));
-    if (lanes < 1) return fail(ORION_E_UNSUPPORTED, "grid line too long for the line kernels");
-    if (d > 0 && lanes >= 8) lanes = lanes / 8 * 8;
-    L.lanes[d] = lanes;
-    std::vector<LineTile> tiles;
-    for (int b = 0; b < nb; ++b) {
-      const auto& h = c->hb[b];
-      const int nlines = d == 0 ? h.jdim * h.kdim : (d == 1 ? h.idim * h.kdim : h.idim * h.jdim);
-      for (int s = 0; s < nlines; s += lanes) tiles.push_back(LineTile{b, s, std::min(lanes, nlines - s), 0});
-    }
-    if ((rc = dev_upload(c, &L.tiles[d], tiles))) return rc;
-    L.n_tiles[d] = (int)tiles.size();
-  }
+  if ((rc = build_line_tiles(c))) return rc;
 
   // wavefront launches: launch t of the forward sweeps covers hyperplane t of
   // every block, launch t of the backward sweeps hyperplane nplanes-1-t.
@@ -868,6 +877,152 @@ int orion_case_set_params(orion_case_t c, const orion_params_t* params) {
     c->graph = nullptr;
   }
   return 0;
+}
+
+static void current_schedule(orion_case_t c, orion_schedule_t* s) {
+  s->sweep_form = c->L.cl_size > 0 ? ORION_SWEEP_CLUSTER : (c->L.persist_grid > 0 ? ORION_SWEEP_GRID : ORION_SWEEP_PLANES);
+  s->cluster_size = c->L.cl_size;
+  s->lanes = c->L.lanes_cap;
+  s->ms_per_step = 0.f;
+}
+
+static int apply_schedule(orion_case_t c, const orion_schedule_t& s) {
+  if (s.lanes < 1 || s.lanes > 32) return fail(ORION_E_INVALID, "lanes must be 1..32");
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  int rc = 0;
+  if (s.lanes != c->L.lanes_cap) {
+    c->L.lanes_cap = s.lanes;
+    if ((rc = build_line_tiles(c))) return rc;
+  }
+  rc = ops_for(c->prec).schedule(c, s.sweep_form, s.cluster_size);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return rc;
+}
+
+int orion_case_set_schedule(orion_case_t c, const orion_schedule_t* s) {
+  if (!c || !s) return fail(ORION_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(g_struct_mu);
+  return apply_schedule(c, *s);
+}
+
+int orion_case_get_schedule(orion_case_t c, orion_schedule_t* s) {
+  if (!c || !s) return fail(ORION_E_INVALID, "null argument");
+  current_schedule(c, s);
+  return 0;
+}
+
+static int launch_steps(orion_case_t c, int nsteps);
+static int sweep_status(orion_case_t c);
+
+int orion_case_autotune(orion_case_t c, int steps_per_trial, orion_schedule_t* trials, int cap, int* ntrials,
+                        orion_schedule_t* best) {
+  if (!c || !ntrials || !best || steps_per_trial < 1 || (cap > 0 && !trials))
+    return fail(ORION_E_INVALID, "bad arguments");
+  if (c->pending_n > 0) return fail(ORION_E_INVALID, "submitted steps have not been polled");
+  *ntrials = 0;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  // the state between steps is prim (every other field is recomputed from it)
+  std::vector<double*> prim(c->nblocks);
+  size_t tot = 0;
+  for (int b = 0; b < c->nblocks; ++b) {
+    void* d;
+    int nc;
+    bool st;
+    int rc = field_info(c, b, ORION_FIELD_PRIM, &d, &nc, &st);
+    if (rc) return rc;
+    prim[b] = static_cast<double*>(d);
+    tot += (size_t)6 * c->hb[b].npad;
+  }
+  double* save = nullptr;
+  if (cudaMallocAsync((void**)&save, tot * sizeof(double), c->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ORION_E_NOMEM, "autotune state copy");
+  }
+  auto copy_state = [&](bool out) -> int {
+    size_t o = 0;
+    for (int b = 0; b < c->nblocks; ++b) {
+      const size_t n = (size_t)6 * c->hb[b].npad;
+      CUDA_TRY(cudaMemcpyAsync(out ? save + o : prim[b], out ? prim[b] : save + o, n * sizeof(double),
+                               cudaMemcpyDeviceToDevice, c->stream));
+      o += n;
+    }
+    return 0;
+  };
+  int counter = 0;
+  CUDA_TRY(cudaMemcpy(&counter, c->L.counter, sizeof(int), cudaMemcpyDeviceToHost));
+  const long long steps_done = c->steps_done, hist_count = c->hist_count;
+  int rc = copy_state(true);
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+
+  auto trial = [&](orion_schedule_t s) -> int {
+    int r;
+    {
+      std::lock_guard<std::mutex> lk(g_struct_mu);
+      r = apply_schedule(c, s);
+    }
+    if (r) return r;
+    if ((r = launch_steps(c, 1))) return r;  // capture + warm-up
+    if ((r = copy_state(false))) return r;
+    CUDA_TRY(cudaEventRecord(e0, c->stream));
+    if ((r = launch_steps(c, steps_per_trial))) return r;
+    CUDA_TRY(cudaEventRecord(e1, c->stream));
+    CUDA_TRY(cudaEventSynchronize(e1));
+    if ((r = sweep_status(c))) return r;
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    if ((r = copy_state(false))) return r;
+    s.ms_per_step = ms / steps_per_trial;
+    if (*ntrials < cap) trials[*ntrials] = s;
+    ++*ntrials;
+    if (best->ms_per_step <= 0.f || s.ms_per_step < best->ms_per_step) *best = s;
+    return 0;
+  };
+  orion_schedule_t start;
+  current_schedule(c, &start);
+  best->ms_per_step = 0.f;
+  // phase 1: grid lines per CTA of the line kernels, with the current sweep form
+  for (int lanes : {8, 16, 32}) {
+    if (rc) break;
+    orion_schedule_t s = start;
+    s.lanes = lanes;
+    rc = trial(s);
+  }
+  // phase 2: every sweep form, with the best lanes
+  const orion_schedule_t forms[4] = {{ORION_SWEEP_CLUSTER, 16, 0, 0.f}, {ORION_SWEEP_CLUSTER, 8, 0, 0.f},
+                                     {ORION_SWEEP_GRID, 0, 0, 0.f}, {ORION_SWEEP_PLANES, 0, 0, 0.f}};
+  for (const auto& f : forms) {
+    if (rc) break;
+    if (f.sweep_form == start.sweep_form && (f.sweep_form != ORION_SWEEP_CLUSTER || f.cluster_size == start.cluster_size))
+      continue;  // timed in phase 1
+    orion_schedule_t s = f;
+    s.lanes = best->lanes;
+    const int r = trial(s);
+    if (r == ORION_E_UNSUPPORTED) continue;  // this device cannot hold that form
+    rc = r;
+  }
+  // keep the fastest; the solution is where it was before tuning
+  if (!rc) {
+    std::lock_guard<std::mutex> lk(g_struct_mu);
+    rc = apply_schedule(c, *best);
+  }
+  if (!rc) rc = copy_state(false);
+  if (!rc) {
+    cudaMemcpyAsync(c->L.counter, &counter, sizeof(int), cudaMemcpyHostToDevice, c->stream);
+    cudaStreamSynchronize(c->stream);
+  }
+  c->steps_done = steps_done;
+  c->hist_count = hist_count;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(save, c->stream);
+  cudaStreamSynchronize(c->stream);
+  return rc;
 }
 
 int orion_case_sync(orion_case_t c) {

@@ -159,12 +159,14 @@ struct Stages {
     return ok;
   }
 
+  // only_cs: 0 = largest co-resident cluster size (16, else 8), else just that size
   template <int NT>
-  static int cluster_setup(orion_case_t c) {
+  static int cluster_setup(orion_case_t c, int only_cs = 0) {
     auto kern = k_sweeps_cluster<S, T, NT>;
     const size_t smem = cluster_smem(c);
     if (smem > kClusterSmemMax || !cluster_attributes<NT>()) return 0;
     for (int cs : {16, 8}) {
+      if (only_cs && cs != only_cs) continue;
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3(cs * 64);
       cfg.blockDim = dim3(NT);
@@ -189,6 +191,42 @@ struct Stages {
     return 0;
   }
 
+  // The cooperative grid form: one CTA pair per SM, all co-resident.
+  static int grid_setup(orion_case_t c) {
+    const int nt = c->L.sweep_nt;
+    int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    if (nt == 512)
+      CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweeps_persistent<S, T, 512>, 512, 0));
+    else
+      CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweeps_persistent<S, T, 256>, 256, 0));
+    const int want = 512 / nt;
+    if (!coop || per_sm < want) return 0;
+    c->L.persist_grid = nsm * want;
+    return 0;
+  }
+
+  // An explicit sweep form (ORION_SWEEP_PLANES / _GRID / _CLUSTER with size cs).
+  static int schedule(orion_case_t c, int form, int cs) {
+    c->L.persist_grid = 0;
+    c->L.cl_size = 0;
+    if (form == ORION_SWEEP_PLANES) return 0;
+    if (form == ORION_SWEEP_GRID) {
+      int rc = grid_setup(c);
+      if (rc) return rc;
+      return c->L.persist_grid > 0 ? 0 : fail(ORION_E_UNSUPPORTED, "cooperative sweep grid not co-resident");
+    }
+    if (form == ORION_SWEEP_CLUSTER) {
+      if (cs != 0 && cs != 8 && cs != 16) return fail(ORION_E_INVALID, "cluster size must be 8 or 16");
+      int rc = c->L.sweep_nt == 512 ? cluster_setup<512>(c, cs) : cluster_setup<256>(c, cs);
+      if (rc) return rc;
+      return c->L.cl_size > 0 ? 0 : fail(ORION_E_UNSUPPORTED, "sweep clusters of that size are not co-resident");
+    }
+    return fail(ORION_E_INVALID, "unknown sweep form");
+  }
+
   static int persistent_grid(orion_case_t c) {
     c->L.persist_grid = 0;
     c->L.cl_size = 0;
@@ -205,18 +243,7 @@ struct Stages {
       if (rc) return rc;
       if (c->L.cl_size > 0) return 0;
     }
-    int dev = 0, coop = 0, nsm = 0, per_sm = 0;
-    CUDA_TRY(cudaGetDevice(&dev));
-    CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    if (nt == 512)
-      CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweeps_persistent<S, T, 512>, 512, 0));
-    else
-      CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweeps_persistent<S, T, 256>, 256, 0));
-    const int want = 512 / nt;
-    if (!coop || per_sm < want) return 0;
-    c->L.persist_grid = nsm * want;
-    return 0;
+    return grid_setup(c);
   }
 
   template <int NT>
@@ -350,6 +377,7 @@ StageOps make_ops() {
   o.init_flow = &X::init_flow;
   o.skew_static = &X::skew_static;
   o.persistent_grid = &X::persistent_grid;
+  o.schedule = &X::schedule;
   return o;
 }
 

@@ -201,6 +201,29 @@ class FlowFieldSet:
     def step_async(self, nsteps: int):
         check(_lib.load().orion_step_async(self._h, nsteps))
 
+    def get_schedule(self) -> dict:
+        s = _lib.Schedule()
+        check(_lib.load().orion_case_get_schedule(self._h, C.byref(s)))
+        return {"sweep": _lib.SWEEP_NAMES[s.sweep_form], "cluster_size": s.cluster_size, "lanes": s.lanes}
+
+    def set_schedule(self, sweep: str, cluster_size: int = 0, lanes: int = 32):
+        """Fixes the step schedule: sweep form (planes | grid | cluster), cluster size
+        (8, 16, 0 = largest co-resident) and grid lines per CTA of the line kernels."""
+        form = {v: k for k, v in _lib.SWEEP_NAMES.items()}[sweep]
+        s = _lib.Schedule(form, cluster_size, lanes, 0.0)
+        check(_lib.load().orion_case_set_schedule(self._h, C.byref(s)))
+
+    def autotune(self, steps_per_trial: int = 3) -> dict:
+        """Times candidate schedules on this case and keeps the fastest; the
+        solution is unchanged.  Returns the chosen schedule and every trial."""
+        trials = (_lib.Schedule * 16)()
+        n = C.c_int()
+        best = _lib.Schedule()
+        check(_lib.load().orion_case_autotune(self._h, steps_per_trial, trials, 16, C.byref(n), C.byref(best)))
+        row = lambda s: {"sweep": _lib.SWEEP_NAMES[s.sweep_form], "cluster_size": s.cluster_size, "lanes": s.lanes,
+                         "ms_per_step": round(float(s.ms_per_step), 4)}
+        return {"best": row(best), "trials": [row(trials[i]) for i in range(min(n.value, 16))]}
+
     def submit(self, nsteps: int):
         """Enqueues nsteps steps and the asynchronous copy of their residual
         history; returns at once (orion_step_submit)."""
