@@ -1320,14 +1320,50 @@ __device__ __forceinline__ void sweep_apply(const BlockDev<S>& B, const ParamsDe
 }
 
 // One hyperplane of one sweep for every block; chunks list contiguous compact ranges.
+// Launched as a programmatic dependent of the previous hyperplane's launch:
+// before griddepcontrol.wait it reads what no earlier hyperplane writes (the
+// neighbour indices, the diagonal coefficient, the RHS) and prefetches its
+// splitting coefficients into L2, so the launch and those DRAM reads overlap
+// the previous hyperplane; after the wait (the previous grid has completed
+// and its writes are visible) it reads the neighbours' increments.  It lets
+// its own dependent launch only after its wait, so at most one hyperplane
+// ahead is resident.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
+
 template <typename S, typename T, int MODE, int NT>
 __global__ void __launch_bounds__(NT) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
                                                     const Chunk* __restrict__ chunks, ParamsDev P) {
   const Chunk ch = chunks[blockIdx.x];
-  if ((int)threadIdx.x >= ch.count) return;
+  const bool active = (int)threadIdx.x < ch.count;
   const BlockDev<S>& B = blocks[ch.block];
   SweepOps<T> o;
-  sweep_fetch<S, T, MODE>(B, ch.block, (int)ch.start + threadIdx.x, o);
+  o.block = -1;
+  const long long nc = B.ncomp;
+  if (active) {
+    const int c = (int)ch.start + threadIdx.x;
+    o.block = ch.block;
+    o.c = c;
+    for (int q = 0; q < 6; ++q) {
+      const bool used = (q < 3) ? (MODE == SW_LUSGS_FWD || MODE == SW_GS) : (MODE == SW_LUSGS_BWD || MODE == SW_GS);
+      o.nb[q] = used ? B.sk_nb[q * nc + c] : -1;
+    }
+    o.coed = (T)B.sk_coed[c];
+    if (MODE != SW_LUSGS_BWD)
+      for (int m = 0; m < 5; ++m) o.own[m] = -(T)B.sk_rhs[m * nc + c];
+    for (int q = 0; q < 6; ++q) {
+      if (o.nb[q] < 0) continue;
+      for (int k = 0; k < 5; ++k) prefetch_l2(B.sk_pair + (long long)(5 * q + k) * nc + c);
+      for (int k = 0; k < 6; ++k) prefetch_l2(B.sk_nbq + (long long)k * nc + o.nb[q]);
+    }
+    for (int k = 0; k < 9; ++k) prefetch_l2(B.sk_nrm + (long long)k * nc + c);
+  }
+  grid_dep_wait();
+  grid_dep_launch();
+  if (!active) return;
+  if (MODE == SW_LUSGS_BWD)  // the forward increment: the launch just before may have written it
+    for (int m = 0; m < 5; ++m) o.own[m] = (T)__ldcg(B.sk_dq + m * nc + o.c);
   sweep_apply<S, T, MODE>(B, P, o);
 }
 

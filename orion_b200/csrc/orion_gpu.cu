@@ -318,8 +318,8 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
       void* dnb = b64 ? (void*)b64->sk_nb : (void*)b32->sk_nb;
       CUDA_TRY(cudaMemcpyAsync(dnb, nbv.data(), nbv.size() * 4, cudaMemcpyHostToDevice, c->stream));
     }
-    // FP32 sweeps fit 512 threads per CTA without spilling, FP64 sweeps 256
-    const int nt = c->prec == ORION_PREC_FP64 ? 256 : 512;
+    // 256 points per sweep chunk (one per thread): more, smaller CTAs per hyperplane
+    const int nt = 256;
     L.sweep_nt = nt;
     for (int dir = 0; dir < 2; ++dir) {
       std::vector<Chunk> ch;
@@ -576,9 +576,11 @@ int dispatch(orion_case_t c, F fn) {
 // retires one case while others run must not do.
 static std::mutex g_ring_mu;
 
-// Case creation and destruction, graph capture and parameter changes are
-// serialised across host threads (a request loop builds cases on one thread
-// while it steps others on another); launches and copies are not.
+// Graph capture, schedule and parameter changes are serialised across host
+// threads (a request loop builds cases on some threads while it steps others
+// on another); case creation, launches and copies are not: each case has its
+// own stream, memory and lists, and process-wide kernel attributes are set
+// once (std::call_once).
 static std::mutex g_struct_mu;
 static std::vector<ResidualOut*> g_free_rings;
 
@@ -731,7 +733,6 @@ size_t orion_footprint_estimate(int nblocks, const orion_block_desc_t* blocks, i
 int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion_params_t* params, int precision,
                       orion_case_t* out) {
   if (!out || !params) return fail(ORION_E_INVALID, "null argument");
-  std::lock_guard<std::mutex> lk(g_struct_mu);
   *out = nullptr;
   if (precision != ORION_PREC_FP64 && precision != ORION_PREC_MIXED) return fail(ORION_E_INVALID, "bad precision");
   int rc = validate_blocks(nblocks, blocks);
@@ -845,7 +846,6 @@ int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion
 int orion_case_destroy(orion_case_t c) {
   if (!c) return 0;
   cudaStreamSynchronize(c->stream);
-  std::lock_guard<std::mutex> lk(g_struct_mu);
   destroy_case(c);
   return 0;
 }

@@ -117,18 +117,34 @@ struct Stages {
     return 0;
   }
 
-  template <int MODE>
-  static void sweep(orion_case_t c, int dir) {
+  // One launch per hyperplane, each a programmatic dependent of the one before
+  // (griddepcontrol in k_sweep_plane), so launch latency and the static loads
+  // of a hyperplane overlap the previous one.
+  template <int MODE, int NT>
+  static int sweep_nt(orion_case_t c, int dir) {
     auto& L = c->L;
     const auto& off = L.sweep_off[dir];
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
     for (int t = 0; t + 1 < (int)off.size(); ++t) {
       const int n = off[t + 1] - off[t];
       if (n <= 0) continue;
-      if (L.sweep_nt == 512)
-        k_sweep_plane<S, T, MODE, 512><<<n, 512, 0, c->stream>>>(blocks(c), L.sweep_chunks[dir] + off[t], c->P);
-      else
-        k_sweep_plane<S, T, MODE, 256><<<n, 256, 0, c->stream>>>(blocks(c), L.sweep_chunks[dir] + off[t], c->P);
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(n);
+      cfg.blockDim = dim3(NT);
+      cfg.stream = c->stream;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweep_plane<S, T, MODE, NT>, blocks(c),
+                                  (const Chunk*)(L.sweep_chunks[dir] + off[t]), c->P));
     }
+    return 0;
+  }
+
+  template <int MODE>
+  static int sweep(orion_case_t c, int dir) {
+    return c->L.sweep_nt == 512 ? sweep_nt<MODE, 512>(c, dir) : sweep_nt<MODE, 256>(c, dir);
   }
 
   // Sweep scheduling.  Preferred: cluster sweeps (16- or 8-CTA clusters, as
@@ -304,10 +320,11 @@ struct Stages {
       int rc = sweeps_persistent(c);
       if (rc) return rc;
     } else {
-      sweep<SW_LUSGS_FWD>(c, 0);
-      sweep<SW_LUSGS_BWD>(c, 1);
-      sweep<SW_GS>(c, 0);
-      sweep<SW_GS>(c, 1);
+      int rc = sweep<SW_LUSGS_FWD>(c, 0);
+      if (!rc) rc = sweep<SW_LUSGS_BWD>(c, 1);
+      if (!rc) rc = sweep<SW_GS>(c, 0);
+      if (!rc) rc = sweep<SW_GS>(c, 1);
+      if (rc) return rc;
     }
     if (fuse_residual) {
       k_sweep_finish<S, true, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,

@@ -121,13 +121,14 @@ class Server:
     """The request loop.  precision: _lib.PREC_MIXED (default) or PREC_FP64."""
 
     def __init__(self, precision: int = _lib.PREC_MIXED, device: int = 0, hbm_budget: Optional[int] = None,
-                 max_active: int = 64, quantum: int = 20, keep_state: bool = False,
+                 max_active: int = 64, quantum: int = 20, keep_state: bool = False, builders: int = 4,
                  clock: Callable[[], float] = time.perf_counter):
         self.precision = precision
         self.device = device
         self.max_active = max_active
         self.quantum = quantum
         self.keep_state = keep_state
+        self.builders = max(1, builders)
         self.clock = clock
         if hbm_budget is None:
             import torch
@@ -154,29 +155,30 @@ class Server:
         active: Dict[int, _Slot] = {}
         results: List[Result] = []
         used = 0
-        building: Optional[tuple] = None  # (future, request, footprint)
-        pool = cf.ThreadPoolExecutor(max_workers=1)
+        building: List[tuple] = []  # (future, request, footprint), oldest first
+        pool = cf.ThreadPoolExecutor(max_workers=self.builders)
         t0 = self.clock()
         try:
             while pending or queue or active or building:
                 now = self.clock() - t0
                 while pending and pending[0].arrival_s <= now:
                     queue.append(pending.popleft())
-                # admission: FIFO, one case being built at a time
-                if building is None and queue and len(active) < self.max_active:
+                # admission: first come first served, up to `builders` cases being built
+                while queue and len(building) < self.builders and len(active) + len(building) < self.max_active:
                     req = queue[0]
                     fp = self.footprint(req)
                     if fp > self.hbm_budget:
                         queue.popleft()
                         results.append(Result(req.rid, req.npoints, req.nblocks, "rejected", 0, 0, req.arrival_s,
                                               now, now, math.nan, math.nan))
-                    elif used + fp <= self.hbm_budget:
-                        queue.popleft()
-                        used += fp
-                        building = (pool.submit(self.make_case, req), req, fp)
-                if building is not None and building[0].done():
-                    fut, req, fp = building
-                    building = None
+                        continue
+                    if used + fp > self.hbm_budget:
+                        break
+                    queue.popleft()
+                    used += fp
+                    building.append((pool.submit(self.make_case, req), req, fp))
+                while building and building[0][0].done():  # in admission order
+                    fut, req, fp = building.pop(0)
                     fs = fut.result()
                     slot = _Slot(req, fs, fp, self.clock() - t0)
                     fs.submit(min(self.quantum, req.max_steps))

@@ -47,6 +47,7 @@ class FakeServer(serving.Server):
         self.log = []
         self.resident = 0
         self.max_resident_bytes = 0
+        kw.setdefault("builders", 1)  # one builder: the admission log is in admission order
         super().__init__(hbm_budget=kw.pop("hbm_budget"), clock=self._clock, **kw)
         self.t = 0.0
 
@@ -96,6 +97,16 @@ def test_admission_respects_hbm_budget_and_arrival_order():
         peak = max(peak, used)
     assert peak <= 100
     assert srv.peak_bytes <= 100
+
+
+def test_parallel_builders_keep_the_budget():
+    sizes = {i: 20 + 10 * (i % 4) for i in range(12)}
+    reqs = [_req(i, 0.0005 * i, decay=0.6) for i in range(12)]
+    srv = FakeServer(sizes, hbm_budget=90, quantum=3, builders=3)
+    res = srv.run(reqs)
+    assert [r.status for r in res] == ["converged"] * 12
+    assert srv.peak_bytes <= 90
+    assert srv.peak_resident >= 2
 
 
 def test_request_larger_than_budget_is_rejected():
