@@ -132,6 +132,7 @@ struct StageOps {
   int (*skew_static)(orion_case_t, int block);
   int (*persistent_grid)(orion_case_t);
   int (*schedule)(orion_case_t, int form, int cluster_size);
+  int (*prim_shadow)(orion_case_t, int block);
 };
 
 // Groups the mesh blocks into `nclusters` clusters (largest first onto the

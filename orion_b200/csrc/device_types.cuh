@@ -22,6 +22,12 @@ struct BlockDev {
   S* mu;
   S* duvwt;               // 12 comps: node derivatives of u,v,w,T along xi,eta,zeta
   const uint8_t* bcmask;  // 1 where a physical-BC window zeroes dq
+  // FP32 shadows the mixed path's flux kernels read (nullptr on the plain path):
+  // prim (6 comps) refreshed by the state kernel after the BCs, metrics (9) and
+  // vol refreshed whenever they are set.  FP64 prim/metrics/vol stay the master.
+  float* prim_f;
+  float* met_f;
+  float* vol_f;
   int ni, nj, nk;         // interior points
   int nx, ny, nz;         // padded
   long long npad;

@@ -12,6 +12,22 @@
 
 namespace orion {
 
+// Arrays the flux kernels read: FP32 shadows on the mixed path (exactly the
+// values its FP32 arithmetic converts the FP64 arrays to), the FP64 arrays on
+// the plain path.
+template <typename S> struct FluxSrc;
+template <> struct FluxSrc<double> {
+  static __device__ __forceinline__ const double* prim(const BlockDev<double>& B) { return B.prim; }
+  static __device__ __forceinline__ const double* metrics(const BlockDev<double>& B) { return B.metrics; }
+  static __device__ __forceinline__ const double* vol(const BlockDev<double>& B) { return B.vol; }
+};
+template <> struct FluxSrc<float> {
+  static __device__ __forceinline__ const float* prim(const BlockDev<float>& B) { return B.prim_f; }
+  static __device__ __forceinline__ const float* metrics(const BlockDev<float>& B) { return B.met_f; }
+  static __device__ __forceinline__ const float* vol(const BlockDev<float>& B) { return B.vol_f; }
+};
+
+
 template <typename S>
 __device__ __forceinline__ long long lin(const BlockDev<S>& B, int i, int j, int k) {
   return (long long)i + (long long)B.nx * ((long long)j + (long long)B.ny * (long long)k);
@@ -345,6 +361,10 @@ __device__ __forceinline__ void state_point(const BlockDev<S>& B, const ParamsDe
     B.mu[idx] = muv;
   }
   for (int m = 0; m < 5; ++m) B.dq[m * np + idx] = (S)0;
+  if (sizeof(S) == 4) {  // the flux kernels' FP32 copy of prim, after the BCs and T
+    for (int m = 0; m < 5; ++m) B.prim_f[m * np + idx] = (float)prim[m * np + idx];
+    B.prim_f[5 * np + idx] = (float)prim[5 * np + idx];
+  }
   c_out = cval;
   mu_out = muv;
 }
@@ -355,13 +375,14 @@ __device__ __forceinline__ S timestep_point(const BlockDev<S>& B, const ParamsDe
   const long long np = B.npad;
   const S u = (S)__ldg(B.prim + np + idx), v = (S)__ldg(B.prim + 2 * np + idx), w = (S)__ldg(B.prim + 3 * np + idx);
   const S rho = (S)__ldg(B.prim + idx);
-  const S vol = (S)__ldg(B.vol + idx);
+  const S vol = (S)__ldg(FluxSrc<S>::vol(B) + idx);
   const S reynolds = (S)P.reynolds, csrv = (S)P.csrv;
   S sum_spec = S(0);
+  const auto* met = FluxSrc<S>::metrics(B);
   for (int d = 0; d < 3; ++d) {
-    const S mx = (S)__ldg(B.metrics + (3 * d + 0) * np + idx);
-    const S my = (S)__ldg(B.metrics + (3 * d + 1) * np + idx);
-    const S mz = (S)__ldg(B.metrics + (3 * d + 2) * np + idx);
+    const S mx = (S)__ldg(met + (3 * d + 0) * np + idx);
+    const S my = (S)__ldg(met + (3 * d + 1) * np + idx);
+    const S mz = (S)__ldg(met + (3 * d + 2) * np + idx);
     const S U_contra = tabs(u * mx + v * my + w * mz);
     const S grad_len = tsqrt(mx * mx + my * my + mz * mz);
     const S spec = U_contra + c * grad_len;
@@ -466,8 +487,8 @@ __global__ void k_timestep(const BlockDev<S>* __restrict__ blocks, const Chunk* 
 // (compute_derivatives_cell + compute_node_deriv_line,
 // src/solver/FluxComputer.cpp:13-67, 301-376).
 // ===========================================================================
-template <typename T>
-__device__ __forceinline__ T node_deriv(const double* __restrict__ q, long long o, long long st, int t, int L,
+template <typename T, typename A>
+__device__ __forceinline__ T node_deriv(const A* __restrict__ q, long long o, long long st, int t, int L,
                                         bool fl, bool fr) {
   // q + o is memory coordinate 0 of the line, st the along-line stride, t the interior index.
   auto Q = [&](int p) -> T { return (T)q[o + (long long)p * st]; };
@@ -510,7 +531,7 @@ __global__ void k_node_derivs(const BlockDev<S>* __restrict__ blocks, const Chun
       const bool fr = B.prim[o + (long long)(L + 5) * st] < 0.0;
       const int comp[4] = {1, 2, 3, 5};
       for (int m = 0; m < 4; ++m) {
-        const T v = node_deriv<T>(B.prim + comp[m] * np, o, st, tt[d], L, fl, fr);
+        const T v = node_deriv<T>(FluxSrc<S>::prim(B) + comp[m] * np, o, st, tt[d], L, fl, fr);
         B.duvwt[(m + 4 * d) * np + idx] = (S)v;
       }
     }
@@ -525,8 +546,8 @@ __global__ void k_node_derivs(const BlockDev<S>* __restrict__ blocks, const Chun
 // One CTA per tile of whole lines: face fluxes to shared memory, then the
 // 6th-order difference and dq -= dfv / Re.
 // ===========================================================================
-template <typename T>
-__device__ __forceinline__ T interp_half(const double* __restrict__ a, long long o, long long st, int f, int L,
+template <typename T, typename A>
+__device__ __forceinline__ T interp_half(const A* __restrict__ a, long long o, long long st, int f, int L,
                                          bool fl, bool fr) {
   // interp_line_to_half at face f of a line of L points; a + o is memory coordinate 0.
   auto Q = [&](int p) -> T { return (T)a[o + (long long)p * st]; };
@@ -543,8 +564,8 @@ __device__ __forceinline__ T interp_half_s(const S* __restrict__ a, long long o,
   return (T(9) * (Q(f + 2) + Q(f + 3)) + T(-1) * (Q(f + 4) + Q(f + 1))) / T(16);
 }
 
-template <typename T>
-__device__ __forceinline__ T half_deriv(const double* __restrict__ a, long long o, long long st, int f, int L, bool fl,
+template <typename T, typename A>
+__device__ __forceinline__ T half_deriv(const A* __restrict__ a, long long o, long long st, int f, int L, bool fl,
                                         bool fr) {
   auto Q = [&](int p) -> T { return (T)a[o + (long long)p * st]; };
   if (fl && f == 0) return (T(-71) * Q(3) + T(141) * Q(4) + T(-93) * Q(5) + T(23) * Q(6)) / T(24);
@@ -570,15 +591,16 @@ __device__ __forceinline__ void viscous_face(const BlockDev<S>& B, const ParamsD
                                              bool fl, bool fr, T cp_prl, T fv[4]) {
   const long long np = B.npad;
   const long long st = stride_along(B, D);
-  const double* prim = B.prim;
+  const auto* prim = FluxSrc<S>::prim(B);
   T uvwt[4];
   const int comp[4] = {1, 2, 3, 5};
   for (int m = 0; m < 4; ++m) uvwt[m] = interp_half<T>(prim + comp[m] * np, o, st, f, L, fl, fr);
   const T vs = interp_half_s<T, S>(B.mu, o, st, f);
   const T kcp = vs * cp_prl;
-  const T volh = interp_half_s<T, double>(B.vol, o, st, f);
+  const T volh = interp_half_s<T, S>(FluxSrc<S>::vol(B), o, st, f);
   T kxyz[9];
-  for (int m = 0; m < 9; ++m) kxyz[m] = interp_half_s<T, double>(B.metrics + m * np, o, st, f);
+  const auto* met = FluxSrc<S>::metrics(B);
+  for (int m = 0; m < 9; ++m) kxyz[m] = interp_half_s<T, S>(met + m * np, o, st, f);
   T d[12];
   // derivative along the line (half point), cross derivatives interpolated
   for (int m = 0; m < 4; ++m) d[m + 4 * D] = half_deriv<T>(prim + comp[m] * np, o, st, f, L, fl, fr);
@@ -697,7 +719,7 @@ __global__ void __launch_bounds__(256, LineMinBlocks<T>::visc) k_viscous(const B
 // ===========================================================================
 template <typename S, typename T>
 struct InvLine {
-  const double* prim;
+  const S* prim;  // FluxSrc<S>::prim
   long long o, st, np;
   int L;
   __device__ __forceinline__ T q(int p, int m) const { return (T)prim[m * np + o + (long long)p * st]; }
@@ -706,7 +728,7 @@ struct InvLine {
 template <typename S, typename T>
 __device__ __forceinline__ T metric_half(const BlockDev<S>& B, int mc, long long o, long long st, int f, int L) {
   // interp_metrics_half (InviscidFluxComputer.cpp:136-192), ni > 2
-  const double* a = B.metrics + mc * B.npad;
+  const S* a = FluxSrc<S>::metrics(B) + mc * B.npad;
   auto Q = [&](int p) -> T { return (T)a[o + (long long)p * st]; };
   if (f == 0) return (T(35) * Q(3) + T(-35) * Q(4) + T(21) * Q(5) + T(-5) * Q(6)) / T(16);
   if (f == 1) return (T(5) * Q(3) + T(15) * Q(4) + T(-5) * Q(5) + T(1) * Q(6)) / T(16);
@@ -935,7 +957,7 @@ __global__ void __launch_bounds__(256, LineMinBlocks<T>::inv) k_inviscid(const B
     int lane, f;
     tile_item<D>(it, tl.count, nf, lane, f);
     const long long o = line_origin(B, D, tl.first + lane);
-    InvLine<S, T> ln{B.prim, o, st, B.npad, L};
+    InvLine<S, T> ln{FluxSrc<S>::prim(B), o, st, B.npad, L};
     const bool fl = B.prim[o] < 1.0e-20;
     const bool fr = B.prim[o + (long long)(L + 5) * st] < 1.0e-20;
     T ql[5], qr[5], kx, ky, kz, fo[5];
@@ -972,7 +994,7 @@ __global__ void __launch_bounds__(256, LineMinBlocks<T>::inv) k_inviscid(const B
     const bool flag = left ? (B.prim[o] < 1.0e-20) : (B.prim[o + (long long)(L + 5) * st] < 1.0e-20);
     if (!flag) continue;
     const int t = left ? slot : L - 6 + slot;
-    InvLine<S, T> ln{B.prim, o, st, B.npad, L};
+    InvLine<S, T> ln{FluxSrc<S>::prim(B), o, st, B.npad, L};
     T fc[5];
     if (left) cascade_left<D, S, T>(B, ln, t, gamma, fc);
     else cascade_right<D, S, T>(B, ln, t, gamma, fc);
@@ -1048,6 +1070,24 @@ __device__ __forceinline__ double sqrt_s(double x) { return sqrt(x); }
 __device__ __forceinline__ float sqrt_s(float x) { return sqrtf(x); }
 
 // Static skewed operands (metrics, vol, unit normals): refreshed whenever they are uploaded.
+// FP32 shadows of one block's metrics and vol (padded, ghosts included).
+static __global__ void k_metric_shadow(const BlockDev<float>* __restrict__ blocks, int b) {
+  const BlockDev<float>& B = blocks[b];
+  const long long np = B.npad;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < np; idx += (long long)gridDim.x * blockDim.x) {
+    for (int m = 0; m < 9; ++m) B.met_f[m * np + idx] = (float)B.metrics[m * np + idx];
+    B.vol_f[idx] = (float)B.vol[idx];
+  }
+}
+
+// FP32 shadow of one block's prim (after an upload or the initial state).
+static __global__ void k_prim_shadow(const BlockDev<float>* __restrict__ blocks, int b) {
+  const BlockDev<float>& B = blocks[b];
+  const long long np = B.npad;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < np; idx += (long long)gridDim.x * blockDim.x)
+    for (int m = 0; m < 6; ++m) B.prim_f[m * np + idx] = (float)B.prim[m * np + idx];
+}
+
 template <typename S>
 __global__ void k_skew_static(const BlockDev<S>* __restrict__ blocks, int b) {
   const BlockDev<S> B = blocks[b];
@@ -1084,8 +1124,9 @@ __global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk
     const int nat = B.sk_nat[c];
     const bool masked = B.bcmask[nat] != 0;
     for (int m = 0; m < 5; ++m) B.sk_rhs[m * nc + c] = masked ? (S)0 : B.dq[m * np + nat];
-    const T rho = (T)B.prim[nat], u = (T)B.prim[np + nat], v = (T)B.prim[2 * np + nat],
-            w = (T)B.prim[3 * np + nat], p = (T)B.prim[4 * np + nat];
+    const S* pr = FluxSrc<S>::prim(B);
+    const T rho = (T)pr[nat], u = (T)pr[np + nat], v = (T)pr[2 * np + nat], w = (T)pr[3 * np + nat],
+            p = (T)pr[4 * np + nat];
     B.sk_prim[c] = (S)rho;
     B.sk_prim[nc + c] = (S)u;
     B.sk_prim[2 * nc + c] = (S)v;

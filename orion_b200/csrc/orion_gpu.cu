@@ -63,6 +63,11 @@ size_t block_bytes(const HostBlock& b, size_t ssz) {
   add(np * ssz);      // mu
   add(12 * np * ssz); // duvwt
   add(np);            // bcmask
+  if (ssz == 4) {     // FP32 shadows: prim 6, metrics 9, vol
+    add(6 * np * 4);
+    add(9 * np * 4);
+    add(np * 4);
+  }
   const size_t nc = (size_t)b.idim * b.jdim * b.kdim;
   const size_t npl = (size_t)(b.idim + b.jdim + b.kdim - 2);
   add((npl * b.kdim + 1) * 4);  // koff
@@ -92,6 +97,12 @@ void carve_block(char* base, const HostBlock& b, BlockDev<S>& d) {
   d.mu = reinterpret_cast<S*>(take(np * sizeof(S)));
   d.duvwt = reinterpret_cast<S*>(take(12 * np * sizeof(S)));
   d.bcmask = reinterpret_cast<uint8_t*>(take(np));
+  d.prim_f = d.met_f = d.vol_f = nullptr;
+  if (sizeof(S) == 4) {  // FP32 shadows of prim, metrics, vol for the mixed path's flux kernels
+    d.prim_f = reinterpret_cast<float*>(take(6 * np * 4));
+    d.met_f = reinterpret_cast<float*>(take(9 * np * 4));
+    d.vol_f = reinterpret_cast<float*>(take(np * 4));
+  }
   const size_t nc = (size_t)b.idim * b.jdim * b.kdim;
   const int npl = b.idim + b.jdim + b.kdim - 2;
   d.nplanes = npl;
@@ -1086,6 +1097,10 @@ int orion_case_upload(orion_case_t c, int block, int field, const double* host) 
     rc = dispatch(c, [&](const StageOps& o) { return o.skew_static(c, block); });
     if (rc) return rc;
   }
+  if (field == ORION_FIELD_PRIM) {
+    rc = dispatch(c, [&](const StageOps& o) { return o.prim_shadow(c, block); });
+    if (rc) return rc;
+  }
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   return 0;
 }
@@ -1150,7 +1165,11 @@ int orion_case_grid_metrics(orion_case_t c, int block, const double* x, const do
 }
 
 int orion_case_init_flow(orion_case_t c, uint64_t seed, double amp) {
-  return dispatch(c, [&](const StageOps& o) { return o.init_flow(c, seed, amp); });
+  return dispatch(c, [&](const StageOps& o) {
+    int rc = o.init_flow(c, seed, amp);
+    for (int b = 0; !rc && b < c->nblocks; ++b) rc = o.prim_shadow(c, b);
+    return rc;
+  });
 }
 
 int orion_exchange_bc(orion_case_t c) {

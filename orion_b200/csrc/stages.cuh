@@ -339,6 +339,14 @@ struct Stages {
 
   static int skew_static(orion_case_t c, int b) {
     k_skew_static<S><<<148 * 4, kThreads, 0, c->stream>>>(blocks(c), b);
+    if constexpr (sizeof(S) == 4)
+      k_metric_shadow<<<148 * 4, kThreads, 0, c->stream>>>(reinterpret_cast<const BlockDev<float>*>(blocks(c)), b);
+    return 0;
+  }
+
+  static int prim_shadow(orion_case_t c, int b) {
+    if constexpr (sizeof(S) == 4)
+      k_prim_shadow<<<148 * 4, kThreads, 0, c->stream>>>(reinterpret_cast<const BlockDev<float>*>(blocks(c)), b);
     return 0;
   }
 
@@ -395,6 +403,7 @@ StageOps make_ops() {
   o.skew_static = &X::skew_static;
   o.persistent_grid = &X::persistent_grid;
   o.schedule = &X::schedule;
+  o.prim_shadow = &X::prim_shadow;
   return o;
 }
 
