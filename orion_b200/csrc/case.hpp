@@ -43,7 +43,7 @@ struct DeviceLists {
   LineTile* tiles[3] = {nullptr, nullptr, nullptr};
   int n_tiles[3] = {0, 0, 0};
   int lanes[3] = {1, 1, 1};
-  int lanes_cap = 32;                            // line tiles: at most this many grid lines per CTA
+  int lanes_cap = 32;                            // line tiles: at most this many grid lines per CTA (set at creation)
   int lmax[3] = {0, 0, 0};
   Chunk* sweep_chunks[2] = {nullptr, nullptr};  // forward / backward hyperplane launches
   std::vector<int> sweep_off[2];                 // host: chunk range of each launch

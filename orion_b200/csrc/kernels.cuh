@@ -1304,21 +1304,16 @@ __device__ __forceinline__ void sweep_fetch(const BlockDev<S>& B, int block, int
 // (compute_flux_splitting from dc on, StateUpdater.cpp:255-264, and the viscous
 // off-diagonal term :334-343 / :410-421), accumulated into rhs0 in the
 // reference's order.
-template <typename S, typename T, int MODE>
-__device__ __forceinline__ void sweep_term(const BlockDev<S>& B, T gm1, int nvis, const SweepOps<T>& o, int q,
-                                           T rhs0[5]) {
-  const long long nc = B.ncomp;
-  const long long n = o.nb[q];
-  const T drm = (T)__ldcg(B.sk_dq + n), dum = (T)__ldcg(B.sk_dq + nc + n), dvm = (T)__ldcg(B.sk_dq + 2 * nc + n),
-          dwm = (T)__ldcg(B.sk_dq + 3 * nc + n), dEm = (T)__ldcg(B.sk_dq + 4 * nc + n);
-  const T um = (T)B.sk_nbq[n], vm = (T)B.sk_nbq[nc + n], wm = (T)B.sk_nbq[2 * nc + n];
-  const T H = (T)B.sk_nbq[3 * nc + n], c2 = (T)B.sk_nbq[4 * nc + n], af = (T)B.sk_nbq[5 * nc + n];
-  const int d = q % 3;
-  const long long c = o.c;
-  const T nx_n = (T)B.sk_nrm[(3 * d) * nc + c], ny_n = (T)B.sk_nrm[(3 * d + 1) * nc + c],
-          nz_n = (T)B.sk_nrm[(3 * d + 2) * nc + c];
-  const S* pc = B.sk_pair + (long long)(5 * q) * nc + c;
-  const T l1 = (T)pc[0], x1 = (T)pc[nc], x2 = (T)pc[2 * nc], ct_n = (T)pc[3 * nc], rvh = (T)pc[4 * nc];
+// The increment-dependent arithmetic of one neighbour term, from its loaded
+// operands (dn: neighbour increment; nq: u, v, w, H, c2, af of the neighbour;
+// pc: l1, x1, x2, ct_n, rv/2 of the pair; nrm: the point's unit normal).
+template <typename T, int MODE>
+__device__ __forceinline__ void split_term(int q, T gm1, int nvis, const T dn[5], const T nq[6], const T pc[5],
+                                           const T nrm[3], T rhs0[5]) {
+  const T drm = dn[0], dum = dn[1], dvm = dn[2], dwm = dn[3], dEm = dn[4];
+  const T um = nq[0], vm = nq[1], wm = nq[2], H = nq[3], c2 = nq[4], af = nq[5];
+  const T nx_n = nrm[0], ny_n = nrm[1], nz_n = nrm[2];
+  const T l1 = pc[0], x1 = pc[1], x2 = pc[2], ct_n = pc[3], rvh = pc[4];
   const T dc = ct_n * drm - (nx_n * dum + ny_n * dvm + nz_n * dwm);
   const T dh = af * drm - gm1 * (um * dum + vm * dvm + wm * dwm - dEm);
   const T c2dc = c2 * dc;
@@ -1328,7 +1323,6 @@ __device__ __forceinline__ void sweep_term(const BlockDev<S>& B, T gm1, int nvis
   fs[2] = l1 * dvm + (ny_n * c2dc - vm * dh) * x1 + (ny_n * dh - vm * dc) * x2;
   fs[3] = l1 * dwm + (nz_n * c2dc - wm * dh) * x1 + (nz_n * dh - wm * dc) * x2;
   fs[4] = l1 * dEm + (ct_n * c2dc - H * dh) * x1 + (ct_n * dh - H * dc) * x2;
-  const T dn[5] = {drm, dum, dvm, dwm, dEm};
   const T sgn = q < 3 ? T(1) : T(-1);
   if (nvis == 1) {
     if (MODE == SW_GS) {
@@ -1342,6 +1336,21 @@ __device__ __forceinline__ void sweep_term(const BlockDev<S>& B, T gm1, int nvis
   } else {
     for (int m = 0; m < 5; ++m) rhs0[m] += fs[m];
   }
+}
+
+template <typename S, typename T, int MODE>
+__device__ __forceinline__ void sweep_term(const BlockDev<S>& B, T gm1, int nvis, const SweepOps<T>& o, int q,
+                                           T rhs0[5]) {
+  const long long nc = B.ncomp;
+  const long long n = o.nb[q];
+  const long long c = o.c;
+  const int d = q % 3;
+  T dn[5], nq[6], pc[5], nrm[3];
+  for (int m = 0; m < 5; ++m) dn[m] = (T)__ldcg(B.sk_dq + m * nc + n);
+  for (int k = 0; k < 6; ++k) nq[k] = (T)B.sk_nbq[k * nc + n];
+  for (int k = 0; k < 3; ++k) nrm[k] = (T)B.sk_nrm[(3 * d + k) * nc + c];
+  for (int k = 0; k < 5; ++k) pc[k] = (T)B.sk_pair[(5 * q + k) * nc + c];
+  split_term<T, MODE>(q, gm1, nvis, dn, nq, pc, nrm, rhs0);
 }
 
 template <typename S, typename T, int MODE>
@@ -1376,36 +1385,81 @@ __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefe
 template <typename S, typename T, int MODE, int NT>
 __global__ void __launch_bounds__(NT) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
                                                     const Chunk* __restrict__ chunks, ParamsDev P) {
+  constexpr int Q0 = MODE == SW_LUSGS_BWD ? 3 : 0;
+  constexpr int Q1 = MODE == SW_LUSGS_FWD ? 3 : 6;
+  constexpr bool PRELOAD = sizeof(T) == 4;  // FP32: every static operand in registers before the wait
   const Chunk ch = chunks[blockIdx.x];
   const bool active = (int)threadIdx.x < ch.count;
   const BlockDev<S>& B = blocks[ch.block];
-  SweepOps<T> o;
-  o.block = -1;
   const long long nc = B.ncomp;
+  const int c = (int)ch.start + threadIdx.x;
+  int nb[6];
+  T coed = T(0), own[5];
+  T nq[6][6], pc[6][5], nrm[3][3];
   if (active) {
-    const int c = (int)ch.start + threadIdx.x;
-    o.block = ch.block;
-    o.c = c;
-    for (int q = 0; q < 6; ++q) {
-      const bool used = (q < 3) ? (MODE == SW_LUSGS_FWD || MODE == SW_GS) : (MODE == SW_LUSGS_BWD || MODE == SW_GS);
-      o.nb[q] = used ? B.sk_nb[q * nc + c] : -1;
-    }
-    o.coed = (T)B.sk_coed[c];
+#pragma unroll
+    for (int q = Q0; q < Q1; ++q) nb[q] = B.sk_nb[q * nc + c];
+    coed = (T)B.sk_coed[c];
     if (MODE != SW_LUSGS_BWD)
-      for (int m = 0; m < 5; ++m) o.own[m] = -(T)B.sk_rhs[m * nc + c];
-    for (int q = 0; q < 6; ++q) {
-      if (o.nb[q] < 0) continue;
-      for (int k = 0; k < 5; ++k) prefetch_l2(B.sk_pair + (long long)(5 * q + k) * nc + c);
-      for (int k = 0; k < 6; ++k) prefetch_l2(B.sk_nbq + (long long)k * nc + o.nb[q]);
+#pragma unroll
+      for (int m = 0; m < 5; ++m) own[m] = -(T)B.sk_rhs[m * nc + c];
+#pragma unroll
+    for (int q = Q0; q < Q1; ++q) {
+      if (nb[q] < 0) continue;
+      if (PRELOAD) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) nq[q][k] = (T)B.sk_nbq[k * nc + nb[q]];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) pc[q][k] = (T)B.sk_pair[(5 * q + k) * nc + c];
+      } else {
+        for (int k = 0; k < 5; ++k) prefetch_l2(B.sk_pair + (long long)(5 * q + k) * nc + c);
+        for (int k = 0; k < 6; ++k) prefetch_l2(B.sk_nbq + (long long)k * nc + nb[q]);
+      }
     }
-    for (int k = 0; k < 9; ++k) prefetch_l2(B.sk_nrm + (long long)k * nc + c);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (PRELOAD) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) nrm[d][k] = (T)B.sk_nrm[(3 * d + k) * nc + c];
+      } else {
+        for (int k = 0; k < 3; ++k) prefetch_l2(B.sk_nrm + (long long)(3 * d + k) * nc + c);
+      }
+    }
   }
   grid_dep_wait();
   grid_dep_launch();
   if (!active) return;
   if (MODE == SW_LUSGS_BWD)  // the forward increment: the launch just before may have written it
-    for (int m = 0; m < 5; ++m) o.own[m] = (T)__ldcg(B.sk_dq + m * nc + o.c);
-  sweep_apply<S, T, MODE>(B, P, o);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) own[m] = (T)__ldcg(B.sk_dq + m * nc + c);
+  // every neighbour increment in flight at once
+  T dn[6][5];
+#pragma unroll
+  for (int q = Q0; q < Q1; ++q)
+    if (nb[q] >= 0)
+#pragma unroll
+      for (int m = 0; m < 5; ++m) dn[q][m] = (T)__ldcg(B.sk_dq + m * nc + nb[q]);
+  const T gm1 = T(P.gamma) - T(1);
+  T rhs0[5] = {T(0), T(0), T(0), T(0), T(0)};
+  // lower neighbours first (i, j, k), then upper (i, j, k): the reference's order
+#pragma unroll
+  for (int q = Q0; q < Q1; ++q) {
+    if (nb[q] < 0) continue;
+    const int d = q % 3;
+    if (!PRELOAD) {
+      for (int k = 0; k < 6; ++k) nq[q][k] = (T)B.sk_nbq[k * nc + nb[q]];
+      for (int k = 0; k < 5; ++k) pc[q][k] = (T)B.sk_pair[(5 * q + k) * nc + c];
+      for (int k = 0; k < 3; ++k) nrm[d][k] = (T)B.sk_nrm[(3 * d + k) * nc + c];
+    }
+    split_term<T, MODE>(q, gm1, P.nvis, dn[q], nq[q], pc[q], nrm[d], rhs0);
+  }
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    S* dst = B.sk_dq + m * nc + c;
+    if (MODE == SW_LUSGS_FWD) *dst = (S)((own[m] + rhs0[m]) * coed);
+    else if (MODE == SW_LUSGS_BWD) *dst = (S)(own[m] - rhs0[m] * coed);
+    else *dst = (S)((rhs0[m] + own[m]) * coed);
+  }
 }
 
 template <typename S, typename T, int MODE>
@@ -1662,31 +1716,37 @@ template <typename S, bool DO_RES, int NT>
 __global__ void __launch_bounds__(NT) k_sweep_finish(const BlockDev<S>* __restrict__ blocks,
                                                      const Chunk* __restrict__ chunks, ParamsDev P,
                                                      ResPartial* __restrict__ partials) {
+  // Natural order (interior index n = i + ni*(j + nj*k)): prim, dq, vol, dt
+  // and the mask are read and written coalesced; only the swept increment is
+  // gathered from the plane-major layout, at c = koff[s*nk + k] + (j - jlo(s,k)).
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
   const long long np = B.npad, nc = B.ncomp;
   double sum = 0.0, mx = -1.0;
   long long key = (long long)0x7fffffffffffffffLL;
   for (int t = threadIdx.x; t < ch.count; t += NT) {
-    const long long c = ch.start + t;
-    const int nat = B.sk_nat[c];
+    const long long n = ch.start + t;
+    const int n32 = (int)n, r32 = n32 / B.ni;
+    const int ii = n32 - r32 * B.ni, jj = r32 % B.nj, kk = r32 / B.nj;
+    const long long idx = lin(B, NG + ii, NG + jj, NG + kk);
+    const int sp = ii + jj + kk;
+    const int jlo = sp - kk - (B.ni - 1) > 0 ? sp - kk - (B.ni - 1) : 0;
+    const long long c = (long long)__ldg(B.koff + (long long)sp * B.nk + kk) + (jj - jlo);
     double dq[5];
-    const bool masked = B.bcmask[nat] != 0;
+    const bool masked = B.bcmask[idx] != 0;
     for (int m = 0; m < 5; ++m) {
-      const S v = masked ? (S)0 : B.sk_dq[m * nc + c];
-      B.dq[m * np + nat] = v;
+      const S v = masked ? (S)0 : __ldcs(B.sk_dq + m * nc + c);
+      B.dq[m * np + idx] = v;
       dq[m] = (double)v;
     }
-    limited_update(B, P, nat, dq);
+    limited_update(B, P, idx, dq);
     if (DO_RES) {
-      double vol = B.vol[nat];
-      double dt = (double)B.dt[nat];
+      double vol = B.vol[idx];
+      double dt = (double)B.dt[idx];
       if (vol < 1e-30) vol = 1e-30;
       if (dt < 1e-30) dt = 1e-30;
       const double inv_factor = 1.0 / (dt * vol);
-      int ii, jj, kk;
-      decode_nat(B, nat, ii, jj, kk);
-      const long long kbase = (B.int_base + ii + (long long)B.ni * (jj + (long long)B.nj * kk)) * 5;
+      const long long kbase = (B.int_base + n) * 5;
       for (int m = 0; m < 5; ++m) {
         const double res = fabs(dq[m]) * inv_factor;
         sum += res * res;

@@ -306,6 +306,8 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
   L.n_int_chunks = (int)itr.size();
   if ((rc = dev_upload(c, &L.pad_base, pad_base))) return rc;
 
+  // line-kernel tiles: 16 grid lines per CTA in FP32, 32 in FP64 (autotuned defaults)
+  L.lanes_cap = c->prec == ORION_PREC_FP64 ? 32 : 16;
   if ((rc = build_line_tiles(c))) return rc;
 
   // wavefront launches: launch t of the forward sweeps covers hyperplane t of

@@ -246,13 +246,13 @@ struct Stages {
   static int persistent_grid(orion_case_t c) {
     c->L.persist_grid = 0;
     c->L.cl_size = 0;
-    // default: clusters for FP32 (co-resident 16-CTA clusters hold 8k threads),
-    // the cooperative grid for FP64 (clusters of 256-thread CTAs hold too few)
+    // default: one programmatic-dependent launch per hyperplane (the fastest
+    // form the autotuner measured on the configurations, both precisions)
     const char* env = getenv("ORION_SWEEP");
-    const std::string mode = env ? std::string(env) : std::string(sizeof(S) == 4 ? "cluster" : "grid");
-    if (mode == "planes") return 0;
-    const char* lim = getenv("ORION_SWEEP_SPIN_LIMIT");
+    const std::string mode = env ? std::string(env) : std::string("planes");
+    const char* lim = getenv("ORION_SWEEP_SPIN_LIMIT");  // bound of the grid barrier's wait
     if (lim) c->L.spin_limit = atoll(lim);
+    if (mode == "planes") return 0;
     const int nt = c->L.sweep_nt;
     if (mode == "cluster") {
       int rc = nt == 512 ? cluster_setup<512>(c) : cluster_setup<256>(c);
