@@ -1552,6 +1552,10 @@ struct SweepSlot {
   int count;
 };
 
+// Static operands of point c: neighbour indices, diagonal coefficient and the
+// RHS (or, backward, the forward increment) into registers; the splitting
+// coefficients, neighbour states and normals prefetched to L2, so that after
+// the barrier only the neighbours' fresh increments miss.
 template <typename S, typename T, int MODE>
 __device__ __forceinline__ void cl_fetch(const SweepBlock<S>& B, int block, int c, SweepOps<T>& o) {
   const long long nc = B.nc;
@@ -1568,57 +1572,41 @@ __device__ __forceinline__ void cl_fetch(const SweepBlock<S>& B, int block, int 
     if (MODE == SW_LUSGS_BWD) o.own[m] = (T)__ldcg(B.dq + m * nc + c);
     else o.own[m] = -(T)B.rhs[m * nc + c];
   }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    if (o.nb[q] < 0) continue;
+    for (int k = 0; k < 5; ++k) prefetch_l2(B.pair + (long long)(5 * q + k) * nc + c);
+    for (int k = 0; k < 6; ++k) prefetch_l2(B.nbq + (long long)k * nc + o.nb[q]);
+  }
+  for (int k = 0; k < 9; ++k) prefetch_l2(B.nrm + (long long)k * nc + c);
 }
 
-template <typename S, typename T, int MODE>
-__device__ __forceinline__ void cl_term(const SweepBlock<S>& B, T gm1, int nvis, const SweepOps<T>& o, int q,
-                                        T rhs0[5]) {
-  const long long nc = B.nc;
-  const long long n = o.nb[q];
-  const T drm = (T)__ldcg(B.dq + n), dum = (T)__ldcg(B.dq + nc + n), dvm = (T)__ldcg(B.dq + 2 * nc + n),
-          dwm = (T)__ldcg(B.dq + 3 * nc + n), dEm = (T)__ldcg(B.dq + 4 * nc + n);
-  const T um = (T)B.nbq[n], vm = (T)B.nbq[nc + n], wm = (T)B.nbq[2 * nc + n];
-  const T H = (T)B.nbq[3 * nc + n], c2 = (T)B.nbq[4 * nc + n], af = (T)B.nbq[5 * nc + n];
-  const int d = q % 3;
-  const long long c = o.c;
-  const T nx_n = (T)B.nrm[(3 * d) * nc + c], ny_n = (T)B.nrm[(3 * d + 1) * nc + c], nz_n = (T)B.nrm[(3 * d + 2) * nc + c];
-  const S* pc = B.pair + (long long)(5 * q) * nc + c;
-  const T l1 = (T)pc[0], x1 = (T)pc[nc], x2 = (T)pc[2 * nc], ct_n = (T)pc[3 * nc], rvh = (T)pc[4 * nc];
-  // compute_flux_splitting from dc on (StateUpdater.cpp:255-264) + viscous term (:334-343 / :410-421)
-  const T dc = ct_n * drm - (nx_n * dum + ny_n * dvm + nz_n * dwm);
-  const T dh = af * drm - gm1 * (um * dum + vm * dvm + wm * dwm - dEm);
-  const T c2dc = c2 * dc;
-  T fs[5];
-  fs[0] = l1 * drm - dh * x1 - dc * x2;
-  fs[1] = l1 * dum + (nx_n * c2dc - um * dh) * x1 + (nx_n * dh - um * dc) * x2;
-  fs[2] = l1 * dvm + (ny_n * c2dc - vm * dh) * x1 + (ny_n * dh - vm * dc) * x2;
-  fs[3] = l1 * dwm + (nz_n * c2dc - wm * dh) * x1 + (nz_n * dh - wm * dc) * x2;
-  fs[4] = l1 * dEm + (ct_n * c2dc - H * dh) * x1 + (ct_n * dh - H * dc) * x2;
-  const T dn[5] = {drm, dum, dvm, dwm, dEm};
-  const T sgn = q < 3 ? T(1) : T(-1);
-  if (nvis == 1) {
-    if (MODE == SW_GS) {
-      for (int m = 0; m < 5; ++m) fs[m] += rvh * dn[m] * sgn;
-    } else {
-      for (int m = 0; m < 5; ++m) fs[m] += rvh * dn[m];
-    }
-  }
-  if (MODE == SW_GS && q >= 3) {
-    for (int m = 0; m < 5; ++m) rhs0[m] -= fs[m];
-  } else {
-    for (int m = 0; m < 5; ++m) rhs0[m] += fs[m];
-  }
-}
-
+// Every neighbour's increment in flight at once, then the terms in the
+// reference's order (split_term: the same arithmetic as the other forms).
 template <typename S, typename T, int MODE>
 __device__ __forceinline__ void cl_apply(const SweepBlock<S>& B, T gm1, int nvis, const SweepOps<T>& o) {
   const long long nc = B.nc;
-  T rhs0[5] = {T(0), T(0), T(0), T(0), T(0)};
+  const long long c = o.c;
+  T dn[6][5];
 #pragma unroll
   for (int q = 0; q < 6; ++q)
-    if (o.nb[q] >= 0) cl_term<S, T, MODE>(B, gm1, nvis, o, q, rhs0);
+    if (o.nb[q] >= 0)
+#pragma unroll
+      for (int m = 0; m < 5; ++m) dn[q][m] = (T)__ldcg(B.dq + m * nc + o.nb[q]);
+  T rhs0[5] = {T(0), T(0), T(0), T(0), T(0)};
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    if (o.nb[q] < 0) continue;
+    const int d = q % 3;
+    T nq[6], pc[5], nrm[3];
+    for (int k = 0; k < 6; ++k) nq[k] = (T)B.nbq[k * nc + o.nb[q]];
+    for (int k = 0; k < 5; ++k) pc[k] = (T)B.pair[(5 * q + k) * nc + c];
+    for (int k = 0; k < 3; ++k) nrm[k] = (T)B.nrm[(3 * d + k) * nc + c];
+    split_term<T, MODE>(q, gm1, nvis, dn[q], nq, pc, nrm, rhs0);
+  }
+#pragma unroll
   for (int m = 0; m < 5; ++m) {
-    S* d = B.dq + m * nc + o.c;
+    S* d = B.dq + m * nc + c;
     if (MODE == SW_LUSGS_FWD) *d = (S)((o.own[m] + rhs0[m]) * o.coed);
     else if (MODE == SW_LUSGS_BWD) *d = (S)(o.own[m] - rhs0[m] * o.coed);
     else *d = (S)((rhs0[m] + o.own[m]) * o.coed);
