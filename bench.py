@@ -47,10 +47,11 @@ STAGE_BYTES = {
 STEP_BYTES = (1912, 1444)
 
 # DRAM bytes per grid point that ncu measured for the update stage's kernels
-# (k_lusgs_prep + k_sweep_pairs + k_sweeps_cluster + k_sweep_finish, mixed
-# path, one launch each on C1 = 1,254,792 points: 208.7 + 218.7 + 919.8 +
-# 131.5 MB); scaled to the bench workload by its point count.
-UPDATE_DRAM_BYTES_PER_POINT_MIXED = 1478.7e6 / 1254792
+# (mixed path, C1 = 1,254,792 points: k_lusgs_prep 176.3 MB + k_sweep_pairs
+# 218.5 MB + the 704 k_sweep_plane launches of one step 1,220.6 MB +
+# k_sweep_finish 118.8 MB; ncu flushes caches per launch, so this is an upper
+# bound); scaled to the bench workload by its point count.
+UPDATE_DRAM_BYTES_PER_POINT_MIXED = 1734.2e6 / 1254792
 
 # The mixed state is compared with the plain FP64 state after this many steps
 # from the same initial state.  On the multi-block configurations the
@@ -282,7 +283,7 @@ def main():
     traffic = None
     if dom == "update_solution":
         traffic = UPDATE_DRAM_BYTES_PER_POINT_MIXED * npts
-        dom = "update_solution (k_lusgs_prep, k_sweep_pairs, k_sweeps_cluster, k_sweep_finish)"
+        dom = "update_solution (k_lusgs_prep, k_sweep_pairs, k_sweep_plane x 4 passes, k_sweep_finish)"
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{peak_kind} hbm_gbs",
                 "bytes_per_point": bpp, "points_per_launch": npts,
