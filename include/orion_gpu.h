@@ -170,6 +170,13 @@ int orion_case_init_flow(orion_case_t c, uint64_t seed, double amp);
  * orion_grid_metrics_host; gcl=1 selects the Visbal conservative form.  Waits. */
 int orion_case_grid_metrics(orion_case_t c, int block, const double* x, const double* y, const double* z, int gcl);
 
+/* Solution output of one block (the fields PostProcess::write_solution
+ * writes, src/postprocess/PostProcess.cpp:116-243): host receives 7 arrays of
+ * idim*jdim*kdim floats, i fastest: density, pressure, temperature, Mach
+ * (sqrt(|u|^2 / (gamma p / rho)) in FP64, 0 where gamma p / rho <= 1e-30),
+ * u, v, w.  Packed on the device, then copied; waits. */
+int orion_case_pack_output(orion_case_t c, int block, float* host);
+
 /* Grid metrics and Jacobian of one block on the host (compute_grid_metrics +
  * check_grid_metrics, src/mesh/MetricComputer.cpp:103-500): x,y,z are
  * idim*jdim*kdim, i fastest; metrics (9 comps) and vol are written in the

@@ -39,6 +39,7 @@
 #include "preprocess/FlowField.hpp"
 #include "preprocess/Inflow.hpp"
 #include "preprocess/InitialCondition.hpp"
+#include "postprocess/PostProcess.hpp"
 #include "solver/FluxComputer.hpp"
 #include "solver/HaloExchanger.hpp"
 #include "solver/InviscidFluxComputer.hpp"
@@ -103,7 +104,7 @@ void dump_state(const std::string& path, const preprocess::FlowFieldSet& fs, dou
 
 int main(int argc, char** argv) {
   if (argc < 4) {
-    std::fprintf(stderr, "usage: %s <case_dir> <nsteps> <out_dir> [--snap-step S] [--time-only]\n", argv[0]);
+    std::fprintf(stderr, "usage: %s <case_dir> <nsteps> <out_dir> [--snap-step S] [--time-only] [--warmup W] [--vts FLOWNAME]\n", argv[0]);
     return 2;
   }
   const std::string dir = argv[1];
@@ -112,11 +113,13 @@ int main(int argc, char** argv) {
   int snap_step = -1;
   bool time_only = false;
   int warmup = 0;
+  std::string vts;  // --vts FLOWNAME: the reference's own solution output after the run
   for (int a = 4; a < argc; ++a) {
     std::string s = argv[a];
     if (s == "--snap-step" && a + 1 < argc) snap_step = std::atoi(argv[++a]);
     else if (s == "--time-only") time_only = true;
     else if (s == "--warmup" && a + 1 < argc) warmup = std::atoi(argv[++a]);
+    else if (s == "--vts" && a + 1 < argc) vts = argv[++a];
 #ifdef ORION_SHIM
     else if (s == "--resident") orion::gpu::set_residency(orion::gpu::Residency::Resident);
     else if (s == "--mixed") orion::gpu::set_mixed_precision(true);
@@ -228,6 +231,10 @@ int main(int argc, char** argv) {
   orion::gpu::sync_to_host(fs);
 #endif
   if (!time_only) dump_state(out + "/final.bin", fs, params.step.phydtime);
+  if (!vts.empty()) {
+    params.filename.flowname = vts;
+    postprocess::PostProcess::write_solution(fs, grid, params, nsteps);
+  }
 
   long long pts = 0;
   for (int nb : fs.local_block_ids) pts += (long long)grid.blocks[nb].npoints();

@@ -56,6 +56,7 @@ SIGNATURES = {
     "orion_case_destroy": (C.c_int, [C.c_void_p]),
     "orion_case_set_params": (C.c_int, [C.c_void_p, C.POINTER(Params)]),
     "orion_step_submit": (C.c_int, [C.c_void_p, C.c_int]),
+    "orion_case_pack_output": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "orion_case_set_schedule": (C.c_int, [C.c_void_p, C.POINTER(Schedule)]),
     "orion_case_get_schedule": (C.c_int, [C.c_void_p, C.POINTER(Schedule)]),
     "orion_case_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Schedule), C.c_int, C.POINTER(C.c_int),

@@ -13,6 +13,7 @@
 
 #include "case.hpp"
 #include "metrics_dev.cuh"
+#include "output_dev.cuh"
 
 using namespace orion;
 
@@ -1163,6 +1164,30 @@ int orion_case_grid_metrics(orion_case_t c, int block, const double* x, const do
   rc = dispatch(c, [&](const StageOps& o) { return o.skew_static(c, block); });
   if (rc) return rc;
   CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int orion_case_pack_output(orion_case_t c, int block, float* host) {
+  if (!c || block < 0 || block >= c->nblocks || !host) return fail(ORION_E_INVALID, "bad arguments");
+  const auto& h = c->hb[block];
+  const long long n = (long long)h.idim * h.jdim * h.kdim;
+  void* dprim;
+  int nc;
+  bool st;
+  int rc = field_info(c, block, ORION_FIELD_PRIM, &dprim, &nc, &st);
+  if (rc) return rc;
+  float* stage = nullptr;
+  if (cudaMallocAsync((void**)&stage, sizeof(float) * 7 * n, c->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ORION_E_NOMEM, "output staging buffer");
+  }
+  out::k_pack_output<<<148 * 4, kThreads, 0, c->stream>>>(static_cast<const double*>(dprim), h.npad, h.idim, h.jdim,
+                                                          h.kdim, h.nx, h.ny, c->P.gamma, stage);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host, stage, sizeof(float) * 7 * n, cudaMemcpyDeviceToHost, c->stream);
+  cudaFreeAsync(stage, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return fail(ORION_E_CUDA, std::string("pack output: ") + cudaGetErrorString(e));
   return 0;
 }
 
