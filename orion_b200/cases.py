@@ -428,6 +428,121 @@ def write_bc_inp(path: str, blocks: Sequence[Block]) -> None:
 
 
 # ---------------------------------------------------------------------------
+# readers of the same formats (case ingestion from the reference's own files)
+# ---------------------------------------------------------------------------
+
+def read_param_dat(path: str):
+    """(FlowParams, nomax) from a Fortran-namelist param.dat (Params.cpp:103-275):
+    `$group` ... `/` blocks of `key = value`; quotes, commas and Fortran `d`
+    exponents are accepted.  Only user-given freestream conditions
+    (height < 0) are supported, as the configurations use."""
+    kv = {}
+    with open(path) as f:
+        for raw in f:
+            line = raw.split("!", 1)[0].strip()
+            if not line or line.startswith("$") or line.startswith("&") or line == "/":
+                continue
+            for part in line.rstrip(",").split(","):
+                if "=" not in part:
+                    continue
+                k, v = part.split("=", 1)
+                kv[k.strip().lower()] = v.strip().strip("'\"")
+
+    def num(key, default, cast=float):
+        if key not in kv:
+            return default
+        return cast(float(kv[key].lower().replace("d", "e")))
+
+    if num("height", -1.0) >= 0.0:
+        raise ValueError("param.dat: height >= 0 (standard-atmosphere conditions) is not supported")
+    p = FlowParams(moo=num("moo", 0.5), reynolds=num("reynolds", 1000.0), cfl=num("cfl", 2.0),
+                   twall=num("twall", 0.0), tref=num("tref", 288.15), pref=num("pref", 101325.0),
+                   attack=num("attack", 0.0), sideslip=num("sideslip", 0.0), nvis=num("nvis", 1, int),
+                   method=num("method", 1, int), ntmst=num("ntmst", 0, int), gcl=num("gcl", 1, int),
+                   csrv=num("csrv", 1, int))
+    return p, num("nomax", 1, int)
+
+
+def _read_records(f):
+    while True:
+        head = f.read(4)
+        if not head:
+            return
+        n = int(np.frombuffer(head, "<u4")[0])
+        payload = f.read(n)
+        if len(payload) != n or f.read(4) != head:
+            raise ValueError("Plot3D: truncated or mismatched Fortran record")
+        yield payload
+
+
+def read_plot3d(path: str) -> List[Block]:
+    """Blocks (coordinates only) from a multi-block Plot3D file in Fortran
+    sequential records, the layout Plot3DReader.cpp:88-156 reads."""
+    with open(path, "rb") as f:
+        recs = _read_records(f)
+        nb = int(np.frombuffer(next(recs), "<i4")[0])
+        dims = [tuple(int(v) for v in np.frombuffer(next(recs), "<i4")) for _ in range(nb)]
+        blocks = []
+        for (ni, nj, nk) in dims:
+            xyz = np.frombuffer(next(recs), "<f8").reshape(3, nk, nj, ni)
+            blocks.append(Block(ni, nj, nk, xyz[0].copy(), xyz[1].copy(), xyz[2].copy(), []))
+    return blocks
+
+
+def read_bc_inp(path: str, blocks: Sequence[Block]) -> None:
+    """Region lists from an ORION BC file (marker 1976, BCReader.cpp:31-182),
+    appended to the blocks in file order.  Index ranges keep their signs (the
+    interface orientation of analyze_bc_connect, BCPreprocess.cpp:16-192)."""
+    with open(path) as f:
+        lines = [ln.strip() for ln in f if ln.strip()]
+    pos = 0
+
+    def ints(n):
+        nonlocal pos
+        v = [int(t) for t in lines[pos].split()]
+        pos += 1
+        if len(v) != n:
+            raise ValueError(f"bc file line {pos}: expected {n} integers")
+        return v
+
+    if int(lines[0]) != 1976:
+        raise ValueError("bc file: marker 1976 expected")
+    pos = 2  # marker, processes in the file
+    nb = ints(1)[0]
+    if nb != len(blocks):
+        raise ValueError(f"bc file: {nb} blocks, grid has {len(blocks)}")
+    for b in blocks:
+        ints(1)  # owning process
+        dims = ints(3)
+        if tuple(dims) != b.dims:
+            raise ValueError(f"bc file: block dims {dims} differ from the grid's {b.dims}")
+        pos += 1  # block name
+        for _ in range(ints(1)[0]):
+            v = ints(7)
+            r = Region((v[0], v[2], v[4]), (v[1], v[3], v[5]), v[6])
+            if v[6] < 0:
+                t = ints(8)
+                r = Region(r.s_st, r.s_ed, v[6], (t[0], t[2], t[4]), (t[1], t[3], t[5]), t[6], t[7])
+            b.regions.append(r)
+
+
+def read_case(path: str, name: Optional[str] = None) -> Case:
+    """A case from a directory in the reference's formats: param.dat, grid.x,
+    bc.inp, and the optional noise.txt (seed, amplitude) of this package."""
+    params, nsteps = read_param_dat(os.path.join(path, "param.dat"))
+    blocks = read_plot3d(os.path.join(path, "grid.x"))
+    read_bc_inp(os.path.join(path, "bc.inp"), blocks)
+    seed, amp = 0, 0.0
+    npath = os.path.join(path, "noise.txt")
+    if os.path.exists(npath):
+        with open(npath) as f:
+            t = f.read().split()
+            seed, amp = int(t[0]), float(t[1])
+    return Case(name or os.path.basename(os.path.normpath(path)), blocks, params, noise_seed=seed,
+                noise_amp=amp, nsteps=nsteps)
+
+
+# ---------------------------------------------------------------------------
 # seeded noise (same sequence as the oracle driver)
 # ---------------------------------------------------------------------------
 
