@@ -1383,7 +1383,7 @@ __device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
 
 template <typename S, typename T, int MODE, int NT>
-__global__ void __launch_bounds__(NT) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
+__global__ void __launch_bounds__(NT, 2) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
                                                     const Chunk* __restrict__ chunks, ParamsDev P) {
   constexpr int Q0 = MODE == SW_LUSGS_BWD ? 3 : 0;
   constexpr int Q1 = MODE == SW_LUSGS_FWD ? 3 : 6;
@@ -1393,6 +1393,12 @@ __global__ void __launch_bounds__(NT) k_sweep_plane(const BlockDev<S>* __restric
   const BlockDev<S>& B = blocks[ch.block];
   const long long nc = B.ncomp;
   const int c = (int)ch.start + threadIdx.x;
+  // pointers into registers now: griddepcontrol.wait clobbers memory, so
+  // anything read through B after it would be reloaded from global memory
+  S* const skdq = B.sk_dq;
+  const S* const sknbq = B.sk_nbq;
+  const S* const skpair = B.sk_pair;
+  const S* const sknrm = B.sk_nrm;
   int nb[6];
   T coed = T(0), own[5];
   T nq[6][6], pc[6][5], nrm[3][3];
@@ -1431,14 +1437,14 @@ __global__ void __launch_bounds__(NT) k_sweep_plane(const BlockDev<S>* __restric
   if (!active) return;
   if (MODE == SW_LUSGS_BWD)  // the forward increment: the launch just before may have written it
 #pragma unroll
-    for (int m = 0; m < 5; ++m) own[m] = (T)__ldcg(B.sk_dq + m * nc + c);
+    for (int m = 0; m < 5; ++m) own[m] = (T)__ldcg(skdq + m * nc + c);
   // every neighbour increment in flight at once
   T dn[6][5];
 #pragma unroll
   for (int q = Q0; q < Q1; ++q)
     if (nb[q] >= 0)
 #pragma unroll
-      for (int m = 0; m < 5; ++m) dn[q][m] = (T)__ldcg(B.sk_dq + m * nc + nb[q]);
+      for (int m = 0; m < 5; ++m) dn[q][m] = (T)__ldcg(skdq + m * nc + nb[q]);
   const T gm1 = T(P.gamma) - T(1);
   T rhs0[5] = {T(0), T(0), T(0), T(0), T(0)};
   // lower neighbours first (i, j, k), then upper (i, j, k): the reference's order
@@ -1447,15 +1453,15 @@ __global__ void __launch_bounds__(NT) k_sweep_plane(const BlockDev<S>* __restric
     if (nb[q] < 0) continue;
     const int d = q % 3;
     if (!PRELOAD) {
-      for (int k = 0; k < 6; ++k) nq[q][k] = (T)B.sk_nbq[k * nc + nb[q]];
-      for (int k = 0; k < 5; ++k) pc[q][k] = (T)B.sk_pair[(5 * q + k) * nc + c];
-      for (int k = 0; k < 3; ++k) nrm[d][k] = (T)B.sk_nrm[(3 * d + k) * nc + c];
+      for (int k = 0; k < 6; ++k) nq[q][k] = (T)sknbq[k * nc + nb[q]];
+      for (int k = 0; k < 5; ++k) pc[q][k] = (T)skpair[(5 * q + k) * nc + c];
+      for (int k = 0; k < 3; ++k) nrm[d][k] = (T)sknrm[(3 * d + k) * nc + c];
     }
     split_term<T, MODE>(q, gm1, P.nvis, dn[q], nq[q], pc[q], nrm[d], rhs0);
   }
 #pragma unroll
   for (int m = 0; m < 5; ++m) {
-    S* dst = B.sk_dq + m * nc + c;
+    S* dst = skdq + m * nc + c;
     if (MODE == SW_LUSGS_FWD) *dst = (S)((own[m] + rhs0[m]) * coed);
     else if (MODE == SW_LUSGS_BWD) *dst = (S)(own[m] - rhs0[m] * coed);
     else *dst = (S)((rhs0[m] + own[m]) * coed);
