@@ -31,6 +31,7 @@ int set_error(int code, const std::string& msg);
 constexpr int kThreads = 256;
 constexpr int kChunk = 256;         // points per CTA (one per thread) for pointwise kernels
 constexpr int kHistCap = 4096;      // residual history ring
+constexpr int kSweepThreads = 256;  // sweep chunks: 256 points, one per thread
 constexpr size_t kLineSmemBudget = 96 * 1024;
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }

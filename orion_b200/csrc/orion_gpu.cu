@@ -333,7 +333,7 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
       CUDA_TRY(cudaMemcpyAsync(dnb, nbv.data(), nbv.size() * 4, cudaMemcpyHostToDevice, c->stream));
     }
     // 256 points per sweep chunk (one per thread): more, smaller CTAs per hyperplane
-    const int nt = 256;
+    const int nt = kSweepThreads;
     L.sweep_nt = nt;
     for (int dir = 0; dir < 2; ++dir) {
       std::vector<Chunk> ch;

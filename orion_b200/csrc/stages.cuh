@@ -144,7 +144,7 @@ struct Stages {
 
   template <int MODE>
   static int sweep(orion_case_t c, int dir) {
-    return c->L.sweep_nt == 512 ? sweep_nt<MODE, 512>(c, dir) : sweep_nt<MODE, 256>(c, dir);
+    return sweep_nt<MODE, kSweepThreads>(c, dir);
   }
 
   // Sweep scheduling.  Preferred: cluster sweeps (16- or 8-CTA clusters, as
@@ -209,16 +209,13 @@ struct Stages {
 
   // The cooperative grid form: one CTA pair per SM, all co-resident.
   static int grid_setup(orion_case_t c) {
-    const int nt = c->L.sweep_nt;
     int dev = 0, coop = 0, nsm = 0, per_sm = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    if (nt == 512)
-      CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweeps_persistent<S, T, 512>, 512, 0));
-    else
-      CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweeps_persistent<S, T, 256>, 256, 0));
-    const int want = 512 / nt;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweeps_persistent<S, T, kSweepThreads>,
+                                                           kSweepThreads, 0));
+    const int want = 2;  // two CTAs per SM
     if (!coop || per_sm < want) return 0;
     c->L.persist_grid = nsm * want;
     return 0;
@@ -236,7 +233,7 @@ struct Stages {
     }
     if (form == ORION_SWEEP_CLUSTER) {
       if (cs != 0 && cs != 8 && cs != 16) return fail(ORION_E_INVALID, "cluster size must be 8 or 16");
-      int rc = c->L.sweep_nt == 512 ? cluster_setup<512>(c, cs) : cluster_setup<256>(c, cs);
+      int rc = cluster_setup<kSweepThreads>(c, cs);
       if (rc) return rc;
       return c->L.cl_size > 0 ? 0 : fail(ORION_E_UNSUPPORTED, "sweep clusters of that size are not co-resident");
     }
@@ -253,9 +250,8 @@ struct Stages {
     const char* lim = getenv("ORION_SWEEP_SPIN_LIMIT");  // bound of the grid barrier's wait
     if (lim) c->L.spin_limit = atoll(lim);
     if (mode == "planes") return 0;
-    const int nt = c->L.sweep_nt;
     if (mode == "cluster") {
-      int rc = nt == 512 ? cluster_setup<512>(c) : cluster_setup<256>(c);
+      int rc = cluster_setup<kSweepThreads>(c);
       if (rc) return rc;
       if (c->L.cl_size > 0) return 0;
     }
@@ -298,14 +294,10 @@ struct Stages {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const long long spin_limit = L.spin_limit;
-    if (L.sweep_nt == 512)
-      CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweeps_persistent<S, T, 512>, blocks(c), (const Chunk*)L.sweep_chunks[0],
-                                  (const int*)L.sweep_off_dev[0], (const Chunk*)L.sweep_chunks[1],
-                                  (const int*)L.sweep_off_dev[1], L.max_planes, c->P, ctl, spin_limit));
-    else
-      CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweeps_persistent<S, T, 256>, blocks(c), (const Chunk*)L.sweep_chunks[0],
-                                  (const int*)L.sweep_off_dev[0], (const Chunk*)L.sweep_chunks[1],
-                                  (const int*)L.sweep_off_dev[1], L.max_planes, c->P, ctl, spin_limit));
+    CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweeps_persistent<S, T, kSweepThreads>, blocks(c),
+                                (const Chunk*)L.sweep_chunks[0], (const int*)L.sweep_off_dev[0],
+                                (const Chunk*)L.sweep_chunks[1], (const int*)L.sweep_off_dev[1], L.max_planes, c->P,
+                                ctl, spin_limit));
     return 0;
   }
 
@@ -314,7 +306,7 @@ struct Stages {
     k_lusgs_prep<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
     k_sweep_pairs<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
     if (L.cl_size > 0) {
-      int rc = L.sweep_nt == 512 ? sweeps_cluster_nt<512>(c) : sweeps_cluster_nt<256>(c);
+      int rc = sweeps_cluster_nt<kSweepThreads>(c);
       if (rc) return rc;
     } else if (L.persist_grid > 0) {
       int rc = sweeps_persistent(c);
