@@ -9,8 +9,9 @@ own CUDA stream in quanta of graph-captured steps (orion_step_submit), so the
 work of all resident cases overlaps on the device.  A case retires at the end
 of the first quantum in which its residual has dropped to `drop` times its
 first-step residual (rms, ResidualMonitor::compute), or after max_steps, or
-when its residual stops being finite; its memory is freed in stream order and
-the next request takes its place.
+as diverged when its residual stops being finite or grows past diverge_growth
+(1e3) times the first step's; its memory is freed in stream order and the
+next request takes its place.
 
 Every case runs on its own stream with its own work lists and the same
 deterministic kernels whatever else is resident, and the quanta are the same,
@@ -121,14 +122,15 @@ class Server:
     """The request loop.  precision: _lib.PREC_MIXED (default) or PREC_FP64."""
 
     def __init__(self, precision: int = _lib.PREC_MIXED, device: int = 0, hbm_budget: Optional[int] = None,
-                 max_active: int = 64, quantum: int = 20, keep_state: bool = False, builders: int = 4,
-                 clock: Callable[[], float] = time.perf_counter):
+                 max_active: int = 256, quantum: int = 20, keep_state: bool = False, builders: int = 4,
+                 diverge_growth: float = 1e3, clock: Callable[[], float] = time.perf_counter):
         self.precision = precision
         self.device = device
         self.max_active = max_active
         self.quantum = quantum
         self.keep_state = keep_state
         self.builders = max(1, builders)
+        self.diverge_growth = diverge_growth
         self.clock = clock
         if hbm_budget is None:
             import torch
@@ -220,7 +222,7 @@ class Server:
         req = slot.req
         status = None
         hit = np.nonzero(rms <= req.drop * rms1)[0]
-        if not np.all(np.isfinite(rms)):
+        if not np.all(np.isfinite(rms)) or np.any(rms > self.diverge_growth * rms1):
             status = "diverged"
         elif hit.size:
             status = "converged"
@@ -281,7 +283,7 @@ def main():
     ap.add_argument("--drop", type=float, default=1e-6)
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--quantum", type=int, default=20)
-    ap.add_argument("--max-active", type=int, default=64)
+    ap.add_argument("--max-active", type=int, default=256)
     ap.add_argument("--baseline", action="store_true", help="also serve one at a time on the plain FP64 path")
     a = ap.parse_args()
     reqs = c4_requests(a.requests, a.seed, a.mean_ms, a.max_steps, a.drop)

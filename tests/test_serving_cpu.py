@@ -4,8 +4,9 @@ The fake case runs `submit`ted steps instantly and reports a residual history
 rms_k = r0 * decay**(k-1) (NaN from step `nan_at` on).  Checks: admission
 never exceeds the HBM budget, requests are admitted first come first served,
 a case retires at the end of the quantum in which its residual dropped to
-`drop` x its first-step residual, at max_steps, or when it stops being
-finite, and a request larger than the whole budget is rejected.
+`drop` x its first-step residual, at max_steps, or as diverged when it stops
+being finite or grows past 1e3 x the first step's, and a request larger than
+the whole budget is rejected.
 """
 import math
 
@@ -73,12 +74,14 @@ def _req(rid, arrival, decay=0.5, nan_at=10 ** 9, max_steps=100):
 def test_retirement_rules_and_quanta():
     reqs = [_req(0, 0.0, decay=0.5),                 # 0.5**10 < 1e-3 at step 11
             _req(1, 0.0, decay=0.99, max_steps=30),  # never drops: stops at max_steps
-            _req(2, 0.0, decay=0.9, nan_at=7)]       # NaN at step 7
-    srv = FakeServer({0: 10, 1: 10, 2: 10}, hbm_budget=100, quantum=5)
+            _req(2, 0.0, decay=0.9, nan_at=7),       # NaN at step 7
+            _req(3, 0.0, decay=1.5)]                 # grows past 1e3 x the first step at step 19
+    srv = FakeServer({0: 10, 1: 10, 2: 10, 3: 10}, hbm_budget=100, quantum=5)
     res = {r.rid: r for r in srv.run(reqs)}
     assert res[0].status == "converged" and res[0].steps_to_drop == 11 and res[0].steps == 15
     assert res[1].status == "max_steps" and res[1].steps == 30
     assert res[2].status == "diverged" and res[2].steps == 10
+    assert res[3].status == "diverged" and res[3].steps == 20
     assert all(r.latency_s > 0 for r in res.values())
 
 
