@@ -33,6 +33,9 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# 32 hardware work queues for the serving run's many streams (read when the
+# CUDA context is made, so set before torch touches the GPU)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 METRIC = "cell-updates/s/GPU plain vs mixed-batched at ≤1e-6 L2 err; p50/p99 solve ms"
 UNIT = "cell-updates/s"

@@ -21,6 +21,14 @@ so a request's result does not depend on the mix it ran in.
 """
 from __future__ import annotations
 
+import os
+
+# Every resident case runs on its own stream.  CUDA maps streams onto a few
+# hardware work queues (8 by default), which serialises independent cases;
+# 32 queues (the maximum) let them overlap.  Read when the CUDA context is
+# made, so it only takes effect if this module is imported first.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 import argparse
 import concurrent.futures as cf
 import json
