@@ -1232,9 +1232,8 @@ __global__ void k_sweep_pairs(const BlockDev<S>* __restrict__ blocks, const Chun
 
 enum SweepMode { SW_LUSGS_FWD = 0, SW_LUSGS_BWD = 1, SW_GS = 2 };
 
-// Neighbour contribution (add_nb / add_nb_contrib, StateUpdater.cpp:326-347, 401-426);
-// cn is the neighbour's compact index, km the current point's metrics for its direction.
-// All four sweeps in one persistent cooperative launch, software-pipelined.
+// The cooperative-grid form (ORION_SWEEP_GRID): all four sweeps in one
+// persistent cooperative launch, software-pipelined.
 // Every CTA walks the hyperplane sequence; for each hyperplane a thread owns at
 // most one point of its CTA's first chunk (further chunks are handled in place).
 // The point's operands that do not change during the sweep (metrics, diagonal
@@ -1695,9 +1694,10 @@ __global__ void __launch_bounds__(NT, 1) k_sweeps_cluster(const BlockDev<S>* __r
   cluster_pass<S, T, SW_GS>(sb, bwd_chunks, bwd_off + base, n, rank, csize, P, slots);
 }
 
-// Finish: zero the physical-BC windows (set_boundary_dq_zero), scatter dq to
-// the natural layout, limited update (update_limited) and, when DO_RES, the
-// residual partials (ResidualMonitor::compute).
+// Finish, per interior point in natural order: zero the physical-BC windows
+// (set_boundary_dq_zero), bring the swept increment back to the natural
+// layout, limited update (update_limited) and, when DO_RES, the residual
+// partials (ResidualMonitor::compute).
 template <typename S>
 __device__ __forceinline__ void limited_update(const BlockDev<S>& B, const ParamsDev& P, long long idx,
                                                const double dq[5]);
