@@ -751,7 +751,11 @@ int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion
   if (precision != ORION_PREC_FP64 && precision != ORION_PREC_MIXED) return fail(ORION_E_INVALID, "bad precision");
   int rc = validate_blocks(nblocks, blocks);
   if (rc) return rc;
-  std::unique_ptr<orion_case_s> c(new orion_case_s());
+  // every early return below releases what was made so far (stream, arena, lists)
+  struct CaseGuard {
+    void operator()(orion_case_s* p) const { destroy_case(p); }
+  };
+  std::unique_ptr<orion_case_s, CaseGuard> c(new orion_case_s());
   c->nblocks = nblocks;
   c->prec = precision;
   CUDA_TRY(cudaGetDevice(&c->device));
@@ -841,16 +845,10 @@ int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion
     CUDA_TRY(cudaMemcpyAsync((void*)dmask, mask.data(), mask.size(), cudaMemcpyHostToDevice, c->stream));
   }
 
-  if ((rc = build_lists(c.get(), prim_off))) {
-    destroy_case(c.release());
-    return rc;
-  }
+  if ((rc = build_lists(c.get(), prim_off))) return rc;
   rc = ops_for(precision).set_attributes();
   if (!rc) rc = ops_for(precision).persistent_grid(c.get());
-  if (rc) {
-    destroy_case(c.release());
-    return rc;
-  }
+  if (rc) return rc;
   // creation-time copies and memsets are ordered on the case's stream
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   *out = c.release();
@@ -1277,6 +1275,19 @@ int orion_step_async(orion_case_t c, int nsteps) {
   return 0;
 }
 
+// Reads the sweep barrier's error flag (the stream is idle).
+static int sweep_status(orion_case_t c) {
+  if (!c->L.sweep_ctl) return 0;
+  int ctl[2] = {0, 0};
+  CUDA_TRY(cudaMemcpy(ctl, c->L.sweep_ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
+  if (ctl[1]) {
+    CUDA_TRY(cudaMemsetAsync(c->L.sweep_ctl, 0, sizeof(ctl), c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return fail(ORION_E_TIMEOUT, "a grid barrier of the implicit sweeps gave up waiting");
+  }
+  return 0;
+}
+
 int orion_step(orion_case_t c, int nsteps, orion_residual_t* hist) {
   if (!c || nsteps < 0) return fail(ORION_E_INVALID, "bad arguments");
   int cnt = 0;
@@ -1288,15 +1299,8 @@ int orion_step(orion_case_t c, int nsteps, orion_residual_t* hist) {
     int rc = launch_steps(c, n);
     if (rc) return rc;
     CUDA_TRY(cudaStreamSynchronize(c->stream));
-    if (c->L.sweep_ctl) {
-      int ctl[2] = {0, 0};
-      CUDA_TRY(cudaMemcpy(ctl, c->L.sweep_ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
-      if (ctl[1]) {
-        CUDA_TRY(cudaMemsetAsync(c->L.sweep_ctl, 0, sizeof(ctl), c->stream));
-        CUDA_TRY(cudaStreamSynchronize(c->stream));
-        return fail(ORION_E_TIMEOUT, "a grid barrier of the implicit sweeps gave up waiting");
-      }
-    }
+    rc = sweep_status(c);
+    if (rc) return rc;
     if (hist) {
       rc = read_hist(c, (long long)cnt + done, n, hist + done);
       if (rc) return rc;
@@ -1305,19 +1309,6 @@ int orion_step(orion_case_t c, int nsteps, orion_residual_t* hist) {
   }
   c->hist_count = (long long)cnt + nsteps;
   CUDA_TRY(cudaGetLastError());
-  return 0;
-}
-
-// Reads the sweep barrier's error flag (the stream is idle).
-static int sweep_status(orion_case_t c) {
-  if (!c->L.sweep_ctl) return 0;
-  int ctl[2] = {0, 0};
-  CUDA_TRY(cudaMemcpy(ctl, c->L.sweep_ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
-  if (ctl[1]) {
-    CUDA_TRY(cudaMemsetAsync(c->L.sweep_ctl, 0, sizeof(ctl), c->stream));
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
-    return fail(ORION_E_TIMEOUT, "a grid barrier of the implicit sweeps gave up waiting");
-  }
   return 0;
 }
 
