@@ -199,7 +199,12 @@ Bound& bind(FlowFieldSet& fs, const bc::BCData* bc, const core::Params* p) {
     b.has_bc = bc != nullptr;
     b.has_params = p != nullptr;
     b.params = a;
-    move(b, fs, kAll, true);
+    try {
+      move(b, fs, kAll, true);
+    } catch (...) {
+      orion_case_destroy(b.h);
+      throw;
+    }
     it = g_bound.emplace(&fs, std::move(b)).first;
   }
   set_params(it->second, p);
