@@ -254,6 +254,53 @@ int orion_case_poll(orion_case_t c, orion_residual_t* out, int cap, int* n);
 int orion_residual_block_noalloc(const double* dq, const double* vol, const double* dt, int idim, int jdim,
                                  int kdim, void* stream, orion_residual_t* out);
 
+/* Block sharding ----------------------------------------------------------
+ * Replaces the MPI call sites of the step (one process per GPU, blocks spread
+ * over the processes, ORION's src/solver/HaloExchanger.cpp:70-179 and :186-398
+ * and the reductions of src/solver/ResidualMonitor.cpp:11-137).
+ * orion_case_create_shard takes the GLOBAL block list, identical on every
+ * shard, and owner[b], the shard (0 .. nshards-1) of global block b; the case
+ * holds the blocks owner[b] == rank, ascending (local block i is global block
+ * global_ids[i], orion_shard_blocks).  Every shard owns at least one block.
+ * A shard steps through the per-stage entry points in OrionSolver::solve's
+ * order, with the two exchanges between shards done by the caller:
+ *   orion_exchange_bc (pairs inside the shard), then for every peer
+ *     orion_shard_pack(HALO) -> send, receive -> orion_shard_unpack(HALO);
+ *   orion_shard_average_begin, for every peer orion_shard_pack(IFACE) -> send,
+ *     receive -> orion_shard_unpack(IFACE), then orion_shard_average_end
+ *     (in place of orion_average_interface_residuals);
+ *   orion_shard_residual, then sum `sum`, take the max of `max` (the smallest
+ *     key among equal maxima) and the min of `dtmin` over the shards:
+ *     rms = sqrt(sum / (5 points)); key / 5 is the global interior point
+ *     (blocks in global order, then k, j, i) and key % 5 the component.
+ * Buffers are FP64 device memory of orion_shard_counts' sizes (doubles); pack
+ * and unpack are enqueued on the case's stream.  The lists of a pair of shards
+ * agree element for element: each shard derives them from the global list.
+ * The graph-captured step, orion_average_interface_residuals and
+ * orion_residual_compute return ORION_E_INVALID on a shard of several. */
+#define ORION_XCHG_HALO 0   /* exchange_bc: primitive elements */
+#define ORION_XCHG_IFACE 1  /* average_interface_residuals: packed dq/vol, 5 per point */
+typedef struct {
+  double sum;       /* sum of squared residuals of the shard's points */
+  double max;       /* largest residual of the shard */
+  long long key;    /* 5 * global interior point + component of the max */
+  double dtmin;     /* min(1000, min dt*vol) of the shard (phydtime) */
+  long long points; /* interior points of ALL shards */
+} orion_shard_residual_t;
+int orion_case_create_shard(int nblocks, const orion_block_desc_t* blocks, const int* owner, int rank,
+                            const orion_params_t* params, int precision, orion_case_t* out);
+int orion_shard_blocks(orion_case_t c, int* nlocal, int* global_ids);
+int orion_shard_counts(orion_case_t c, int kind, int peer, long long* nsend, long long* nrecv);
+int orion_shard_pack(orion_case_t c, int kind, int peer, double* buf);
+int orion_shard_unpack(orion_case_t c, int kind, int peer, const double* buf);
+int orion_shard_average_begin(orion_case_t c);
+int orion_shard_average_end(orion_case_t c);
+int orion_shard_residual(orion_case_t c, orion_shard_residual_t* out); /* waits */
+/* Host only (no device use): the doubles shard `rank` sends to and receives
+ * from every shard, nsend[s] / nrecv[s] for s in 0 .. max(owner). */
+int orion_shard_plan_counts(int nblocks, const orion_block_desc_t* blocks, const int* owner, int rank, int kind,
+                            long long* nsend, long long* nrecv);
+
 #ifdef __cplusplus
 }
 #endif

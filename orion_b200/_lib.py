@@ -47,6 +47,14 @@ class Residual(C.Structure):
                 ("phydtime", C.c_double)]
 
 
+XCHG_HALO, XCHG_IFACE = 0, 1
+
+
+class ShardResidual(C.Structure):
+    _fields_ = [("sum", C.c_double), ("max", C.c_double), ("key", C.c_longlong), ("dtmin", C.c_double),
+                ("points", C.c_longlong)]
+
+
 # every symbol the header declares, with its signature
 SIGNATURES = {
     "orion_last_error": (C.c_char_p, []),
@@ -90,6 +98,18 @@ SIGNATURES = {
     "orion_last_residual": (C.c_int, [C.c_void_p, C.POINTER(Residual)]),
     "orion_residual_block_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                                C.c_void_p, C.POINTER(Residual)]),
+    "orion_case_create_shard": (C.c_int, [C.c_int, C.POINTER(BlockDesc), C.POINTER(C.c_int), C.c_int,
+                                          C.POINTER(Params), C.c_int, C.POINTER(C.c_void_p)]),
+    "orion_shard_blocks": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "orion_shard_counts": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_longlong),
+                                     C.POINTER(C.c_longlong)]),
+    "orion_shard_pack": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "orion_shard_unpack": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "orion_shard_average_begin": (C.c_int, [C.c_void_p]),
+    "orion_shard_average_end": (C.c_int, [C.c_void_p]),
+    "orion_shard_residual": (C.c_int, [C.c_void_p, C.POINTER(ShardResidual)]),
+    "orion_shard_plan_counts": (C.c_int, [C.c_int, C.POINTER(BlockDesc), C.POINTER(C.c_int), C.c_int, C.c_int,
+                                          C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
 }
 
 _lib = None

@@ -9,6 +9,7 @@
 
 #include "device_types.cuh"
 #include "orion_gpu.h"
+#include "exchange_plan.hpp"
 #include "topology.hpp"
 
 namespace orion {
@@ -83,6 +84,22 @@ struct DeviceLists {
   unsigned long long* dtmin = nullptr;
   double* dt_part = nullptr;  // per-CTA minima of dt_phys
   long long* pad_base = nullptr;
+  ResPartial* res_total = nullptr;  // the last residual's raw sum, max and key (shards reduce these)
+};
+
+// Block sharding: a case holding the blocks of one shard, and the device lists
+// of its exchanges with every other shard (exchange_plan.hpp).
+struct ShardLists {
+  int rank = 0;
+  int nranks = 1;
+  std::vector<int> global_ids;          // global block id of each local block
+  std::vector<long long> pad_base;      // global padded offset of each local block (initial noise)
+  long long total_interior_global = 0;  // interior points of every shard
+  std::vector<long long*> halo_send, halo_recv;  // per peer: arena offsets (FP64 elements)
+  std::vector<long long> n_halo_send, n_halo_recv;
+  std::vector<int*> iface_send;         // per peer: own slots
+  std::vector<long long> n_iface_send;
+  std::vector<int> iface_recv_base, iface_recv_n;
 };
 
 }  // namespace orion
@@ -102,6 +119,7 @@ struct orion_case_s {
   std::vector<orion::BlockDev<float>> bd32;
   void* d_blocks = nullptr;
   orion::DeviceLists L;
+  orion::ShardLists shard;
   long long total_interior = 0;
   cudaGraphExec_t graph = nullptr;
   long long steps_done = 0;
@@ -125,6 +143,8 @@ struct StageOps {
   int (*timestep)(orion_case_t);
   int (*viscous)(orion_case_t);
   int (*average)(orion_case_t);
+  int (*average_begin)(orion_case_t);  // pack own interface slots
+  int (*average_end)(orion_case_t);    // average every receiving point
   int (*inviscid)(orion_case_t);
   int (*update)(orion_case_t, bool fuse_residual);
   int (*residual)(orion_case_t);

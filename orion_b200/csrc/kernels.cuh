@@ -1895,7 +1895,7 @@ __global__ void __launch_bounds__(1024) k_res_final(const BlockDev<S>* __restric
                                                      const ResPartial* __restrict__ partials, int npart,
                                                      long long total_points, const unsigned long long* dtmin_bits,
                                                      ResidualOut* __restrict__ hist, int* __restrict__ counter,
-                                                     int capacity) {
+                                                     int capacity, ResPartial* __restrict__ total) {
   double sum = 0.0, mx = -1.0;
   long long key = (long long)0x7fffffffffffffffLL;
   for (int t = threadIdx.x; t < npart; t += 1024) {
@@ -1904,6 +1904,7 @@ __global__ void __launch_bounds__(1024) k_res_final(const BlockDev<S>* __restric
   }
   block_reduce_res<1024>(sum, mx, key);
   if (threadIdx.x == 0) {
+    if (total) *total = ResPartial{sum, mx, key};
     ResidualOut r;
     r.rms = total_points > 0 ? sqrt(sum / (double)total_points) : 0.0;
     r.max = mx;

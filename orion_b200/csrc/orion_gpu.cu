@@ -14,6 +14,7 @@
 #include "case.hpp"
 #include "metrics_dev.cuh"
 #include "output_dev.cuh"
+#include "shard_dev.cuh"
 
 using namespace orion;
 
@@ -285,17 +286,13 @@ int build_line_tiles(orion_case_t c) {
   return 0;
 }
 
-int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
+int build_lists(orion_case_t c, const std::vector<long long>& prim_off, const ExchangePlan& plan) {
   auto& L = c->L;
   const int nb = c->nblocks;
   // pointwise chunks over padded and interior index spaces
   std::vector<Chunk> pad, itr;
-  std::vector<long long> pad_base(nb);
-  long long pb = 0;
   for (int b = 0; b < nb; ++b) {
     const auto& h = c->hb[b];
-    pad_base[b] = pb;
-    pb += h.npad;
     for (long long s = 0; s < h.npad; s += kChunk) pad.push_back(Chunk{b, (int)std::min<long long>(kChunk, h.npad - s), s});
     const long long ni = (long long)h.idim * h.jdim * h.kdim;
     for (long long s = 0; s < ni; s += kChunk) itr.push_back(Chunk{b, (int)std::min<long long>(kChunk, ni - s), s});
@@ -305,7 +302,7 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
   L.n_pad_chunks = (int)pad.size();
   if ((rc = dev_upload(c, &L.int_chunks, itr))) return rc;
   L.n_int_chunks = (int)itr.size();
-  if ((rc = dev_upload(c, &L.pad_base, pad_base))) return rc;
+  if ((rc = dev_upload(c, &L.pad_base, c->shard.pad_base))) return rc;
 
   // line-kernel tiles: 16 grid lines per CTA in FP32, 32 in FP64 (autotuned defaults)
   L.lanes_cap = c->prec == ORION_PREC_FP64 ? 32 : 16;
@@ -356,67 +353,34 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
   }
 
   // ---------------- halo copy (exchange_bc) ----------------
+  // pairs inside this case as arena offsets; pairs with other shards as gather
+  // (send) and scatter (receive) lists per peer
   {
-    struct Msg {
-      int tb, tw;
-      std::vector<long long> src;
-    };
-    std::vector<Msg> queue;
-    for (int b = 0; b < nb; ++b) {
-      const auto& h = c->hb[b];
-      const int dims[3] = {h.idim, h.jdim, h.kdim};
-      for (const auto& hr : h.regions) {
-        if (hr.r.nbt <= 0) continue;
-        int beg[3], end[3];
-        memory_window(hr, NG, dims, 0, beg, end);
-        Msg msg{hr.r.nbt - 1, hr.r.ibcwin - 1, {}};
-        for (int m = 0; m < 5; ++m)
-          for (int k = beg[2]; k <= end[2]; ++k)
-            for (int j = beg[1]; j <= end[1]; ++j)
-              for (int i = beg[0]; i <= end[0]; ++i)
-                msg.src.push_back(prim_off[b] + m * h.npad + (i + (long long)h.nx * (j + (long long)h.ny * k)));
-        queue.push_back(std::move(msg));
-      }
-    }
-    // last writer wins; destinations in order of first appearance.  Dense per
-    // block (slot of each padded prim element), so building it is O(points).
+    auto off = [&](const ElemRef& e) { return prim_off[e.block] + e.elem; };
     std::vector<long long> hs, hd;
-    std::vector<int> slot;
-    for (int b = 0; b < nb; ++b) {
-      const auto& h = c->hb[b];
-      const int dims[3] = {h.idim, h.jdim, h.kdim};
-      slot.assign((size_t)5 * h.npad, -1);
-      for (int r = 0; r < (int)h.regions.size(); ++r) {
-        const auto& hr = h.regions[r];
-        if (hr.r.nbt <= 0) continue;
-        auto it = std::find_if(queue.begin(), queue.end(), [&](const Msg& q) { return q.tb == b && q.tw == r; });
-        if (it == queue.end())
-          return fail(ORION_E_INVALID, "interface block " + std::to_string(b) + " region " + std::to_string(r) +
-                                           " has no sending partner");
-        int beg[3], end[3];
-        memory_window(hr, NG, dims, 1, beg, end);
-        std::vector<long long> pts;
-        for (int k = beg[2]; k <= end[2]; ++k)
-          for (int j = beg[1]; j <= end[1]; ++j)
-            for (int i = beg[0]; i <= end[0]; ++i) pts.push_back(i + (long long)h.nx * (j + (long long)h.ny * k));
-        const size_t np = pts.size();
-        for (size_t q = 0; q < 5 * np && q < it->src.size(); ++q) {
-          const long long local = (long long)(q / np) * h.npad + pts[q % np];
-          int& sl = slot[(size_t)local];
-          if (sl < 0) {
-            sl = (int)hd.size();
-            hd.push_back(prim_off[b] + local);
-            hs.push_back(it->src[q]);
-          } else {
-            hs[(size_t)sl] = it->src[q];
-          }
-        }
-        queue.erase(it);
-      }
+    hs.reserve(plan.halo_src.size());
+    hd.reserve(plan.halo_dst.size());
+    for (size_t q = 0; q < plan.halo_dst.size(); ++q) {
+      hd.push_back(off(plan.halo_dst[q]));
+      hs.push_back(off(plan.halo_src[q]));
     }
     if ((rc = dev_upload(c, &L.halo_src, hs))) return rc;
     if ((rc = dev_upload(c, &L.halo_dst, hd))) return rc;
     L.n_halo = (int)hd.size();
+    auto& X = c->shard;
+    X.halo_send.assign(plan.nranks, nullptr);
+    X.halo_recv.assign(plan.nranks, nullptr);
+    X.n_halo_send.assign(plan.nranks, 0);
+    X.n_halo_recv.assign(plan.nranks, 0);
+    for (int r = 0; r < plan.nranks; ++r) {
+      std::vector<long long> snd, rcv;
+      for (const auto& e : plan.halo_send[r]) snd.push_back(off(e));
+      for (const auto& e : plan.halo_recv[r]) rcv.push_back(off(e));
+      if ((rc = dev_upload(c, &X.halo_send[r], snd))) return rc;
+      if ((rc = dev_upload(c, &X.halo_recv[r], rcv))) return rc;
+      X.n_halo_send[r] = (long long)snd.size();
+      X.n_halo_recv[r] = (long long)rcv.size();
+    }
   }
 
   // ---------------- physical BC phases ----------------
@@ -467,103 +431,33 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off) {
   }
 
   // ---------------- interface residual averaging ----------------
+  // own slots are packed here; the slots of other shards arrive after them
   {
-    struct Src {
-      int slot_base, n;
-    };
-    std::map<std::pair<int, int>, Src> qsrc;  // target (block, region) -> packing region
-    std::vector<int> pkb;
-    std::vector<long long> pki;
-    for (int b = 0; b < nb; ++b) {
-      const auto& h = c->hb[b];
-      for (int r = 0; r < (int)h.regions.size(); ++r) {
-        const auto& g = h.regions[r].r;
-        if (g.bctype >= 0) continue;
-        int lo[3], hi[3];
-        for (int d = 0; d < 3; ++d) {
-          lo[d] = std::min(std::abs(g.s_st[d]), std::abs(g.s_ed[d]));
-          hi[d] = std::max(std::abs(g.s_st[d]), std::abs(g.s_ed[d]));
-        }
-        Src s{(int)pkb.size(), 0};
-        for (int k = lo[2]; k <= hi[2]; ++k)
-          for (int j = lo[1]; j <= hi[1]; ++j)
-            for (int i = lo[0]; i <= hi[0]; ++i) {
-              pkb.push_back(b);
-              pki.push_back((i - 1 + NG) + (long long)h.nx * ((j - 1 + NG) + (long long)h.ny * (k - 1 + NG)));
-              s.n++;
-            }
-        qsrc[{g.nbt - 1, g.ibcwin - 1}] = s;
-      }
+    if ((rc = dev_upload(c, &L.pk_block, plan.pk_block))) return rc;
+    if ((rc = dev_upload(c, &L.pk_idx, plan.pk_idx))) return rc;
+    L.n_pack = (int)plan.pk_block.size();
+    if ((rc = dev_alloc(c, &L.pack, (size_t)plan.n_slots * 5))) return rc;
+    if ((rc = dev_upload(c, &L.ap_block, plan.ap_block))) return rc;
+    if ((rc = dev_upload(c, &L.ap_idx, plan.ap_idx))) return rc;
+    if ((rc = dev_upload(c, &L.ap_off, plan.ap_off))) return rc;
+    if ((rc = dev_upload(c, &L.ap_slot, plan.ap_slot))) return rc;
+    L.n_ap = (int)plan.ap_block.size();
+    auto& X = c->shard;
+    X.iface_send.assign(plan.nranks, nullptr);
+    X.n_iface_send.assign(plan.nranks, 0);
+    for (int r = 0; r < plan.nranks; ++r) {
+      if ((rc = dev_upload(c, &X.iface_send[r], plan.iface_send[r]))) return rc;
+      X.n_iface_send[r] = (long long)plan.iface_send[r].size();
     }
-    // one entry per destination point, partners in region order; dense per block
-    std::vector<int> apb, apo{0}, aps;
-    std::vector<long long> api;
-    std::vector<int> eid;
-    std::vector<std::vector<int>> eslots;
-    for (int b = 0; b < nb; ++b) {
-      const auto& h = c->hb[b];
-      eid.assign((size_t)h.npad, -1);
-      eslots.clear();
-      std::vector<long long> eidx;
-      for (int r = 0; r < (int)h.regions.size(); ++r) {
-        const auto& hr = h.regions[r];
-        const auto& g = hr.r;
-        if (g.bctype >= 0) continue;
-        auto it = qsrc.find({b, r});
-        if (it == qsrc.end())
-          return fail(ORION_E_INVALID, "interface block " + std::to_string(b) + " region " + std::to_string(r) +
-                                           " receives no averaging data");
-        std::vector<std::array<int, 3>> img;
-        int md[3];
-        interface_image(hr, img, md);
-        int slo[3], tlo[3], thi[3];
-        for (int d = 0; d < 3; ++d) {
-          slo[d] = std::min(std::abs(g.s_st[d]), std::abs(g.s_ed[d]));
-          tlo[d] = std::min(std::abs(g.t_st[d]), std::abs(g.t_ed[d]));
-          thi[d] = std::max(std::abs(g.t_st[d]), std::abs(g.t_ed[d]));
-        }
-        const int nxt = thi[0] - tlo[0] + 1, nyt = thi[1] - tlo[1] + 1;
-        for (int k = 0; k < md[2]; ++k)
-          for (int j = 0; j < md[1]; ++j)
-            for (int i = 0; i < md[0]; ++i) {
-              const auto& t = img[(size_t)i + (size_t)md[0] * ((size_t)j + (size_t)md[1] * k)];
-              const long long rem =
-                  (long long)(t[0] - tlo[0]) + (long long)nxt * ((t[1] - tlo[1]) + (long long)nyt * (t[2] - tlo[2]));
-              if (rem < 0 || rem >= it->second.n)
-                return fail(ORION_E_UNSUPPORTED, "interface averaging map leaves the partner window");
-              const long long idx = (slo[0] + i - 1 + NG) +
-                                    (long long)h.nx * ((slo[1] + j - 1 + NG) + (long long)h.ny * (slo[2] + k - 1 + NG));
-              int& e = eid[(size_t)idx];
-              if (e < 0) {
-                e = (int)eslots.size();
-                eslots.emplace_back();
-                eidx.push_back(idx);
-              }
-              eslots[(size_t)e].push_back(it->second.slot_base + (int)rem);
-            }
-      }
-      for (size_t e = 0; e < eslots.size(); ++e) {
-        apb.push_back(b);
-        api.push_back(eidx[e]);
-        for (int sl : eslots[e]) aps.push_back(sl);
-        apo.push_back((int)aps.size());
-      }
-    }
-    if ((rc = dev_upload(c, &L.pk_block, pkb))) return rc;
-    if ((rc = dev_upload(c, &L.pk_idx, pki))) return rc;
-    L.n_pack = (int)pkb.size();
-    if ((rc = dev_alloc(c, &L.pack, (size_t)L.n_pack * 5))) return rc;
-    if ((rc = dev_upload(c, &L.ap_block, apb))) return rc;
-    if ((rc = dev_upload(c, &L.ap_idx, api))) return rc;
-    if ((rc = dev_upload(c, &L.ap_off, apo))) return rc;
-    if ((rc = dev_upload(c, &L.ap_slot, aps))) return rc;
-    L.n_ap = (int)apb.size();
+    X.iface_recv_base = plan.iface_recv_base;
+    X.iface_recv_n = plan.iface_recv_n;
   }
 
   if ((rc = dev_alloc(c, &L.partials, (size_t)L.n_int_chunks))) return rc;
   if ((rc = dev_alloc(c, &L.hist, (size_t)kHistCap))) return rc;
   if ((rc = dev_alloc(c, &L.counter, 1))) return rc;
   if ((rc = dev_alloc(c, &L.dtmin, 1))) return rc;
+  if ((rc = dev_alloc(c, &L.res_total, 1))) return rc;
   if ((rc = dev_alloc(c, &L.dt_part, (size_t)std::max(L.n_pad_chunks, L.n_int_chunks)))) return rc;
   {
     int* ctl = nullptr;
@@ -710,6 +604,150 @@ static void set_params_dev(ParamsDev& P, const orion_params_t& p) {
   P.method = p.method;
 }
 
+// Host blocks of a descriptor list, regions classified.
+static int host_blocks(int nblocks, const orion_block_desc_t* blocks, std::vector<HostBlock>& hb) {
+  hb.assign(nblocks, HostBlock{});
+  for (int b = 0; b < nblocks; ++b) {
+    auto& h = hb[b];
+    h.idim = blocks[b].idim;
+    h.jdim = blocks[b].jdim;
+    h.kdim = blocks[b].kdim;
+    h.nx = h.idim + 2 * NG;
+    h.ny = h.jdim + 2 * NG;
+    h.nz = h.kdim + 2 * NG;
+    h.npad = (long long)h.nx * h.ny * h.nz;
+    const int dims[3] = {h.idim, h.jdim, h.kdim};
+    for (int r = 0; r < blocks[b].nregions; ++r) {
+      HostRegion hr;
+      hr.r = blocks[b].regions[r];
+      classify_region(hr, dims);
+      if (hr.r.bctype < 0 && hr.s_nd == 0) return fail(ORION_E_INVALID, "interface region is not a plane");
+      h.regions.push_back(hr);
+    }
+  }
+  return 0;
+}
+
+// A case of the blocks `owner[b] == rank` of the global list (owner NULL: all
+// blocks, rank 0).  Residual keys and the initial noise use global block
+// offsets, so every shard's blocks are numbered as in the whole case.
+static int create_case(int nglobal, const orion_block_desc_t* blocks, const int* owner, int rank,
+                       const orion_params_t* params, int precision, orion_case_t* out) {
+  if (!out || !params) return fail(ORION_E_INVALID, "null argument");
+  *out = nullptr;
+  if (precision != ORION_PREC_FP64 && precision != ORION_PREC_MIXED) return fail(ORION_E_INVALID, "bad precision");
+  int rc = validate_blocks(nglobal, blocks);
+  if (rc) return rc;
+  std::vector<HostBlock> gb;
+  if ((rc = host_blocks(nglobal, blocks, gb))) return rc;
+  ExchangePlan plan;
+  {
+    const std::vector<int> own = owner ? std::vector<int>(owner, owner + nglobal) : std::vector<int>();
+    const std::string err = build_exchange_plan(gb, own, rank, plan, NG);
+    if (!err.empty()) return fail(ORION_E_INVALID, err);
+  }
+  if (plan.local.empty()) return fail(ORION_E_INVALID, "shard " + std::to_string(rank) + " owns no block");
+  const int nblocks = (int)plan.local.size();
+  // every early return below releases what was made so far (stream, arena, lists)
+  struct CaseGuard {
+    void operator()(orion_case_s* p) const { destroy_case(p); }
+  };
+  std::unique_ptr<orion_case_s, CaseGuard> c(new orion_case_s());
+  c->nblocks = nblocks;
+  c->prec = precision;
+  CUDA_TRY(cudaGetDevice(&c->device));
+  set_params_dev(c->P, *params);
+  // The case's own stream first: its memory is allocated and freed in stream
+  // order on it, so making or freeing a case never waits for other cases' work.
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(ORION_E_CUDA, "cudaStreamCreate");
+  c->own_stream = true;
+
+  // global offsets of every block's interior and padded points
+  std::vector<long long> gint(nglobal), gpad(nglobal);
+  long long ti = 0, tp = 0;
+  for (int g = 0; g < nglobal; ++g) {
+    gint[g] = ti;
+    gpad[g] = tp;
+    ti += (long long)gb[g].idim * gb[g].jdim * gb[g].kdim;
+    tp += gb[g].npad;
+  }
+  auto& X = c->shard;
+  X.rank = plan.rank;
+  X.nranks = plan.nranks;
+  X.global_ids = plan.local;
+  X.total_interior_global = ti;
+  long long tot = 0;
+  for (int g : plan.local) {
+    c->hb.push_back(gb[g]);
+    X.pad_base.push_back(gpad[g]);
+    tot += (long long)gb[g].idim * gb[g].jdim * gb[g].kdim;
+  }
+  c->total_interior = tot;
+
+  // arena
+  const size_t ssz = precision == ORION_PREC_FP64 ? 8 : 4;
+  std::vector<size_t> boff(nblocks);
+  size_t total = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    boff[b] = total;
+    total += block_bytes(c->hb[b], ssz);
+  }
+  if (cudaMallocAsync(&c->arena, total, c->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ORION_E_NOMEM, "device arena of " + std::to_string(total) + " bytes");
+  }
+  c->arena_bytes = total;
+  CUDA_TRY(cudaMemsetAsync(c->arena, 0, total, c->stream));
+  std::vector<long long> prim_off(nblocks);
+  if (precision == ORION_PREC_FP64) {
+    c->bd64.resize(nblocks);
+    for (int b = 0; b < nblocks; ++b) {
+      carve_block(static_cast<char*>(c->arena) + boff[b], c->hb[b], c->bd64[b]);
+      c->bd64[b].int_base = gint[plan.local[b]];
+      prim_off[b] = (c->bd64[b].prim - static_cast<double*>(c->arena));
+    }
+    CUDA_TRY(cudaMallocAsync(&c->d_blocks, sizeof(BlockDev<double>) * nblocks, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->d_blocks, c->bd64.data(), sizeof(BlockDev<double>) * nblocks, cudaMemcpyHostToDevice,
+                             c->stream));
+  } else {
+    c->bd32.resize(nblocks);
+    for (int b = 0; b < nblocks; ++b) {
+      carve_block(static_cast<char*>(c->arena) + boff[b], c->hb[b], c->bd32[b]);
+      c->bd32[b].int_base = gint[plan.local[b]];
+      prim_off[b] = (c->bd32[b].prim - static_cast<double*>(c->arena));
+    }
+    CUDA_TRY(cudaMallocAsync(&c->d_blocks, sizeof(BlockDev<float>) * nblocks, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->d_blocks, c->bd32.data(), sizeof(BlockDev<float>) * nblocks, cudaMemcpyHostToDevice,
+                             c->stream));
+  }
+
+  // physical-BC dq mask (set_boundary_dq_zero windows, StateUpdater.cpp:447-468)
+  for (int b = 0; b < nblocks; ++b) {
+    const auto& h = c->hb[b];
+    std::vector<uint8_t> mask((size_t)h.npad, 0);
+    for (const auto& hr : h.regions) {
+      if (hr.r.bctype <= 0) continue;
+      for (int k = hr.r.s_st[2] - 1 + NG; k <= hr.r.s_ed[2] - 1 + NG; ++k)
+        for (int j = hr.r.s_st[1] - 1 + NG; j <= hr.r.s_ed[1] - 1 + NG; ++j)
+          for (int i = hr.r.s_st[0] - 1 + NG; i <= hr.r.s_ed[0] - 1 + NG; ++i)
+            if (i >= 0 && j >= 0 && k >= 0 && i < h.nx && j < h.ny && k < h.nz)
+              mask[(size_t)i + (size_t)h.nx * ((size_t)j + (size_t)h.ny * k)] = 1;
+    }
+    const uint8_t* dmask = precision == ORION_PREC_FP64 ? c->bd64[b].bcmask : c->bd32[b].bcmask;
+    CUDA_TRY(cudaMemcpyAsync((void*)dmask, mask.data(), mask.size(), cudaMemcpyHostToDevice, c->stream));
+  }
+
+  if ((rc = build_lists(c.get(), prim_off, plan))) return rc;
+  rc = ops_for(precision).set_attributes();
+  if (!rc) rc = ops_for(precision).persistent_grid(c.get());
+  if (rc) return rc;
+  // creation-time copies and memsets are ordered on the case's stream
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  *out = c.release();
+  return 0;
+}
+
 extern "C" {
 
 const char* orion_last_error(void) { return g_last_error.c_str(); }
@@ -746,113 +784,13 @@ size_t orion_footprint_estimate(int nblocks, const orion_block_desc_t* blocks, i
 
 int orion_case_create(int nblocks, const orion_block_desc_t* blocks, const orion_params_t* params, int precision,
                       orion_case_t* out) {
-  if (!out || !params) return fail(ORION_E_INVALID, "null argument");
-  *out = nullptr;
-  if (precision != ORION_PREC_FP64 && precision != ORION_PREC_MIXED) return fail(ORION_E_INVALID, "bad precision");
-  int rc = validate_blocks(nblocks, blocks);
-  if (rc) return rc;
-  // every early return below releases what was made so far (stream, arena, lists)
-  struct CaseGuard {
-    void operator()(orion_case_s* p) const { destroy_case(p); }
-  };
-  std::unique_ptr<orion_case_s, CaseGuard> c(new orion_case_s());
-  c->nblocks = nblocks;
-  c->prec = precision;
-  CUDA_TRY(cudaGetDevice(&c->device));
-  set_params_dev(c->P, *params);
-  // The case's own stream first: its memory is allocated and freed in stream
-  // order on it, so making or freeing a case never waits for other cases' work.
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
-    return fail(ORION_E_CUDA, "cudaStreamCreate");
-  c->own_stream = true;
+  return create_case(nblocks, blocks, nullptr, 0, params, precision, out);
+}
 
-  c->hb.resize(nblocks);
-  long long tot = 0;
-  for (int b = 0; b < nblocks; ++b) {
-    auto& h = c->hb[b];
-    h.idim = blocks[b].idim;
-    h.jdim = blocks[b].jdim;
-    h.kdim = blocks[b].kdim;
-    h.nx = h.idim + 2 * NG;
-    h.ny = h.jdim + 2 * NG;
-    h.nz = h.kdim + 2 * NG;
-    h.npad = (long long)h.nx * h.ny * h.nz;
-    const int dims[3] = {h.idim, h.jdim, h.kdim};
-    for (int r = 0; r < blocks[b].nregions; ++r) {
-      HostRegion hr;
-      hr.r = blocks[b].regions[r];
-      classify_region(hr, dims);
-      if (hr.r.bctype < 0 && hr.s_nd == 0) return fail(ORION_E_INVALID, "interface region is not a plane");
-      h.regions.push_back(hr);
-    }
-    tot += (long long)h.idim * h.jdim * h.kdim;
-  }
-  c->total_interior = tot;
-
-  // arena
-  const size_t ssz = precision == ORION_PREC_FP64 ? 8 : 4;
-  std::vector<size_t> boff(nblocks);
-  size_t total = 0;
-  for (int b = 0; b < nblocks; ++b) {
-    boff[b] = total;
-    total += block_bytes(c->hb[b], ssz);
-  }
-  if (cudaMallocAsync(&c->arena, total, c->stream) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(ORION_E_NOMEM, "device arena of " + std::to_string(total) + " bytes");
-  }
-  c->arena_bytes = total;
-  CUDA_TRY(cudaMemsetAsync(c->arena, 0, total, c->stream));
-  std::vector<long long> prim_off(nblocks);
-  long long ib = 0;
-  if (precision == ORION_PREC_FP64) {
-    c->bd64.resize(nblocks);
-    for (int b = 0; b < nblocks; ++b) {
-      carve_block(static_cast<char*>(c->arena) + boff[b], c->hb[b], c->bd64[b]);
-      c->bd64[b].int_base = ib;
-      ib += (long long)c->hb[b].idim * c->hb[b].jdim * c->hb[b].kdim;
-      prim_off[b] = (c->bd64[b].prim - static_cast<double*>(c->arena));
-    }
-    CUDA_TRY(cudaMallocAsync(&c->d_blocks, sizeof(BlockDev<double>) * nblocks, c->stream));
-    CUDA_TRY(cudaMemcpyAsync(c->d_blocks, c->bd64.data(), sizeof(BlockDev<double>) * nblocks, cudaMemcpyHostToDevice,
-                             c->stream));
-  } else {
-    c->bd32.resize(nblocks);
-    for (int b = 0; b < nblocks; ++b) {
-      carve_block(static_cast<char*>(c->arena) + boff[b], c->hb[b], c->bd32[b]);
-      c->bd32[b].int_base = ib;
-      ib += (long long)c->hb[b].idim * c->hb[b].jdim * c->hb[b].kdim;
-      prim_off[b] = (c->bd32[b].prim - static_cast<double*>(c->arena));
-    }
-    CUDA_TRY(cudaMallocAsync(&c->d_blocks, sizeof(BlockDev<float>) * nblocks, c->stream));
-    CUDA_TRY(cudaMemcpyAsync(c->d_blocks, c->bd32.data(), sizeof(BlockDev<float>) * nblocks, cudaMemcpyHostToDevice,
-                             c->stream));
-  }
-
-  // physical-BC dq mask (set_boundary_dq_zero windows, StateUpdater.cpp:447-468)
-  for (int b = 0; b < nblocks; ++b) {
-    const auto& h = c->hb[b];
-    std::vector<uint8_t> mask((size_t)h.npad, 0);
-    for (const auto& hr : h.regions) {
-      if (hr.r.bctype <= 0) continue;
-      for (int k = hr.r.s_st[2] - 1 + NG; k <= hr.r.s_ed[2] - 1 + NG; ++k)
-        for (int j = hr.r.s_st[1] - 1 + NG; j <= hr.r.s_ed[1] - 1 + NG; ++j)
-          for (int i = hr.r.s_st[0] - 1 + NG; i <= hr.r.s_ed[0] - 1 + NG; ++i)
-            if (i >= 0 && j >= 0 && k >= 0 && i < h.nx && j < h.ny && k < h.nz)
-              mask[(size_t)i + (size_t)h.nx * ((size_t)j + (size_t)h.ny * k)] = 1;
-    }
-    const uint8_t* dmask = precision == ORION_PREC_FP64 ? c->bd64[b].bcmask : c->bd32[b].bcmask;
-    CUDA_TRY(cudaMemcpyAsync((void*)dmask, mask.data(), mask.size(), cudaMemcpyHostToDevice, c->stream));
-  }
-
-  if ((rc = build_lists(c.get(), prim_off))) return rc;
-  rc = ops_for(precision).set_attributes();
-  if (!rc) rc = ops_for(precision).persistent_grid(c.get());
-  if (rc) return rc;
-  // creation-time copies and memsets are ordered on the case's stream
-  CUDA_TRY(cudaStreamSynchronize(c->stream));
-  *out = c.release();
-  return 0;
+int orion_case_create_shard(int nblocks, const orion_block_desc_t* blocks, const int* owner, int rank,
+                            const orion_params_t* params, int precision, orion_case_t* out) {
+  if (!owner) return fail(ORION_E_INVALID, "null owner list");
+  return create_case(nblocks, blocks, owner, rank, params, precision, out);
 }
 
 int orion_case_destroy(orion_case_t c) {
@@ -1213,6 +1151,8 @@ int orion_compute_viscous_rhs(orion_case_t c) {
   return dispatch(c, [&](const StageOps& o) { return o.viscous(c); });
 }
 int orion_average_interface_residuals(orion_case_t c) {
+  if (c && c->shard.nranks > 1)
+    return fail(ORION_E_INVALID, "a shard averages with orion_shard_average_begin, the exchange and orion_shard_average_end");
   return dispatch(c, [&](const StageOps& o) { return o.average(c); });
 }
 int orion_compute_inviscid_rhs(orion_case_t c) {
@@ -1239,6 +1179,7 @@ static int read_hist(orion_case_t c, long long first, int n, orion_residual_t* o
 
 int orion_residual_compute(orion_case_t c, orion_residual_t* out) {
   if (!c || !out) return fail(ORION_E_INVALID, "null argument");
+  if (c->shard.nranks > 1) return fail(ORION_E_INVALID, "a shard's residual is orion_shard_residual, reduced over the shards");
   int cnt = 0;
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   CUDA_TRY(cudaMemcpy(&cnt, c->L.counter, sizeof(int), cudaMemcpyDeviceToHost));
@@ -1260,6 +1201,8 @@ int orion_phydtime(orion_case_t c, double* out) {
 }
 
 static int launch_steps(orion_case_t c, int nsteps) {
+  if (c->shard.nranks > 1)
+    return fail(ORION_E_INVALID, "a shard steps through the per-stage entry points and the shard exchanges");
   int rc = ensure_graph(c);
   if (rc) return rc;
   for (int s = 0; s < nsteps; ++s) CUDA_TRY(cudaGraphLaunch(c->graph, c->stream));
@@ -1377,6 +1320,123 @@ int orion_last_residual(orion_case_t c, orion_residual_t* out) {
   CUDA_TRY(cudaMemcpy(&cnt, c->L.counter, sizeof(int), cudaMemcpyDeviceToHost));
   if (cnt <= 0) return fail(ORION_E_INVALID, "no step has run");
   return read_hist(c, cnt - 1, 1, out);
+}
+
+// ---------------------------------------------------------------------------
+// Block sharding (exchange_plan.hpp): one case per shard, exchanges by buffer.
+// ---------------------------------------------------------------------------
+int orion_shard_blocks(orion_case_t c, int* nlocal, int* global_ids) {
+  if (!c || !nlocal) return fail(ORION_E_INVALID, "null argument");
+  *nlocal = c->nblocks;
+  if (global_ids) std::copy(c->shard.global_ids.begin(), c->shard.global_ids.end(), global_ids);
+  return 0;
+}
+
+static int shard_peer(orion_case_t c, int kind, int peer) {
+  if (!c) return fail(ORION_E_INVALID, "null case");
+  if (kind != ORION_XCHG_HALO && kind != ORION_XCHG_IFACE) return fail(ORION_E_INVALID, "bad exchange kind");
+  if (peer < 0 || peer >= c->shard.nranks || peer == c->shard.rank) return fail(ORION_E_INVALID, "bad peer shard");
+  return 0;
+}
+
+int orion_shard_counts(orion_case_t c, int kind, int peer, long long* nsend, long long* nrecv) {
+  if (!nsend || !nrecv) return fail(ORION_E_INVALID, "null argument");
+  int rc = shard_peer(c, kind, peer);
+  if (rc) return rc;
+  const auto& X = c->shard;
+  if (kind == ORION_XCHG_HALO) {
+    *nsend = X.n_halo_send[peer];
+    *nrecv = X.n_halo_recv[peer];
+  } else {
+    *nsend = 5 * X.n_iface_send[peer];
+    *nrecv = 5 * (long long)X.iface_recv_n[peer];
+  }
+  return 0;
+}
+
+int orion_shard_pack(orion_case_t c, int kind, int peer, double* buf) {
+  int rc = shard_peer(c, kind, peer);
+  if (rc) return rc;
+  const auto& X = c->shard;
+  const long long n = kind == ORION_XCHG_HALO ? X.n_halo_send[peer] : X.n_iface_send[peer];
+  if (n == 0) return 0;
+  if (!buf) return fail(ORION_E_INVALID, "null buffer");
+  const long long work = kind == ORION_XCHG_HALO ? n : 5 * n;
+  const int grid = (int)((work + kThreads - 1) / kThreads);
+  if (kind == ORION_XCHG_HALO)
+    k_shard_gather<<<grid, kThreads, 0, c->stream>>>(static_cast<const double*>(c->arena), X.halo_send[peer], buf, n);
+  else
+    k_shard_gather_slots<<<grid, kThreads, 0, c->stream>>>(c->L.pack, X.iface_send[peer], buf, n);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int orion_shard_unpack(orion_case_t c, int kind, int peer, const double* buf) {
+  int rc = shard_peer(c, kind, peer);
+  if (rc) return rc;
+  const auto& X = c->shard;
+  if (kind == ORION_XCHG_HALO) {
+    const long long n = X.n_halo_recv[peer];
+    if (n == 0) return 0;
+    if (!buf) return fail(ORION_E_INVALID, "null buffer");
+    k_shard_scatter<<<(int)((n + kThreads - 1) / kThreads), kThreads, 0, c->stream>>>(
+        static_cast<double*>(c->arena), X.halo_recv[peer], buf, n);
+    CUDA_TRY(cudaGetLastError());
+  } else {
+    const long long n = X.iface_recv_n[peer];
+    if (n == 0) return 0;
+    if (!buf) return fail(ORION_E_INVALID, "null buffer");
+    CUDA_TRY(cudaMemcpyAsync(c->L.pack + (long long)X.iface_recv_base[peer] * 5, buf, sizeof(double) * 5 * n,
+                             cudaMemcpyDeviceToDevice, c->stream));
+  }
+  return 0;
+}
+
+int orion_shard_average_begin(orion_case_t c) {
+  return dispatch(c, [&](const StageOps& o) { return o.average_begin(c); });
+}
+int orion_shard_average_end(orion_case_t c) {
+  return dispatch(c, [&](const StageOps& o) { return o.average_end(c); });
+}
+
+int orion_shard_residual(orion_case_t c, orion_shard_residual_t* out) {
+  if (!c || !out) return fail(ORION_E_INVALID, "null argument");
+  int rc = dispatch(c, [&](const StageOps& o) { return o.residual(c); });
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  ResPartial t{};
+  unsigned long long bits = 0;
+  CUDA_TRY(cudaMemcpy(&t, c->L.res_total, sizeof(t), cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(&bits, c->L.dtmin, sizeof(bits), cudaMemcpyDeviceToHost));
+  out->sum = t.sum;
+  out->max = t.max;
+  out->key = t.key;
+  std::memcpy(&out->dtmin, &bits, sizeof(double));
+  out->points = c->shard.total_interior_global;
+  return 0;
+}
+
+int orion_shard_plan_counts(int nblocks, const orion_block_desc_t* blocks, const int* owner, int rank, int kind,
+                            long long* nsend, long long* nrecv) {
+  if (!owner || !nsend || !nrecv) return fail(ORION_E_INVALID, "null argument");
+  if (kind != ORION_XCHG_HALO && kind != ORION_XCHG_IFACE) return fail(ORION_E_INVALID, "bad exchange kind");
+  int rc = validate_blocks(nblocks, blocks);
+  if (rc) return rc;
+  std::vector<HostBlock> gb;
+  if ((rc = host_blocks(nblocks, blocks, gb))) return rc;
+  ExchangePlan plan;
+  const std::string err = build_exchange_plan(gb, std::vector<int>(owner, owner + nblocks), rank, plan, NG);
+  if (!err.empty()) return fail(ORION_E_INVALID, err);
+  for (int r = 0; r < plan.nranks; ++r) {
+    if (kind == ORION_XCHG_HALO) {
+      nsend[r] = (long long)plan.halo_send[r].size();
+      nrecv[r] = (long long)plan.halo_recv[r].size();
+    } else {
+      nsend[r] = 5 * (long long)plan.iface_send[r].size();
+      nrecv[r] = 5 * (long long)plan.iface_recv_n[r];
+    }
+  }
+  return 0;
 }
 
 }  // extern "C"

@@ -107,14 +107,25 @@ struct Stages {
     return 0;
   }
 
-  static int average(orion_case_t c) {
+  static int average_begin(orion_case_t c) {
     auto& L = c->L;
     if (L.n_pack == 0) return 0;
     k_iface_pack<S><<<(L.n_pack + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(blocks(c), L.pk_block, L.pk_idx,
                                                                                        L.pack, L.n_pack);
+    return 0;
+  }
+
+  static int average_end(orion_case_t c) {
+    auto& L = c->L;
+    if (L.n_ap == 0) return 0;
     k_iface_apply<S><<<(L.n_ap + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(
         blocks(c), L.ap_block, L.ap_idx, L.ap_off, L.ap_slot, L.pack, L.n_ap);
     return 0;
+  }
+
+  static int average(orion_case_t c) {
+    average_begin(c);
+    return average_end(c);
   }
 
   // One launch per hyperplane, each a programmatic dependent of the one before
@@ -345,7 +356,7 @@ struct Stages {
   static void residual_final(orion_case_t c) {
     auto& L = c->L;
     k_res_final<S><<<1, 1024, 0, c->stream>>>(blocks(c), c->nblocks, L.partials, L.n_int_chunks, c->total_interior * 5,
-                                              L.dtmin, L.hist, L.counter, kHistCap);
+                                              L.dtmin, L.hist, L.counter, kHistCap, L.res_total);
   }
 
   static int residual(orion_case_t c) {
@@ -387,6 +398,8 @@ StageOps make_ops() {
   o.timestep = &X::timestep;
   o.viscous = &X::viscous;
   o.average = &X::average;
+  o.average_begin = &X::average_begin;
+  o.average_end = &X::average_end;
   o.inviscid = &X::inviscid;
   o.update = &X::update;
   o.residual = &X::residual;
