@@ -176,9 +176,12 @@ class Shard:
         return a
 
 
-def _device_buffer(n: int, device: int):
+def _device_buffer(n: int, device):
+    """FP64 buffer of n values on CUDA device `device` (an int), or on the
+    device torch names by a string ("cpu" for gloo)."""
     import torch
-    return torch.empty(max(n, 1), dtype=torch.float64, device=f"cuda:{device}")
+    dev = f"cuda:{device}" if isinstance(device, int) else device
+    return torch.empty(max(n, 1), dtype=torch.float64, device=dev)
 
 
 class LocalTransport:
@@ -217,19 +220,22 @@ class DistTransport:
     """One shard per process over torch.distributed point-to-point: every rank
     posts its sends and receives to every peer together (batch_isend_irecv),
     so the order of ranks cannot deadlock.  The packs finish before the
-    transfer starts and the transfer before the unpacks."""
+    transfer starts and the transfer before the unpacks.  Buffers live on the
+    shard's GPU (NCCL); `buffer_device="cpu"` keeps them in host memory for a
+    gloo group."""
 
-    def __init__(self, group=None):
+    def __init__(self, group=None, buffer_device=None):
         import torch.distributed as dist
         self.dist = dist
         self.group = group
+        self.buffer_device = buffer_device
         self._bufs: Dict[Tuple[int, int, str], object] = {}
 
     def _buf(self, kind: int, peer: int, side: str, n: int, device: int):
         key = (kind, peer, side)
         b = self._bufs.get(key)
         if b is None or b.numel() < n:
-            b = self._bufs[key] = _device_buffer(n, device)
+            b = self._bufs[key] = _device_buffer(n, self.buffer_device or device)
         return b
 
     def exchange(self, shards: Sequence[Shard], kind: int):
@@ -252,12 +258,14 @@ class DistTransport:
         if ops:
             for req in self.dist.batch_isend_irecv(ops):
                 req.wait()
-        torch.cuda.synchronize(s.device)
+        if self.buffer_device is None:
+            torch.cuda.synchronize(s.device)
         for peer, b in recvs:
             s.unpack(kind, peer, b.data_ptr())
 
     def reduce(self, shards: Sequence[Shard], parts) -> List[Tuple[float, float, int, float]]:
-        return gather_partials(parts[0], self.dist, self.group, device=f"cuda:{shards[0].device}")
+        dev = self.buffer_device or f"cuda:{shards[0].device}"
+        return gather_partials(parts[0], self.dist, self.group, device=dev)
 
 
 def gather_partials(part: Tuple[float, float, int, float], dist, group=None, device: str = "cpu"):

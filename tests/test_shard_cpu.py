@@ -11,6 +11,9 @@
   of the same partials: maximum with the smallest key among ties, key decoded
   to the global block and point.
 * partition: contiguous runs, every shard non-empty, points balanced.
+* DistTransport over gloo (world size 3, host buffers, stand-in shards):
+  every rank's sends arrive at the right peer, complete and in order, for
+  both exchanges and with the buffers reused.
 """
 import os
 import socket
@@ -167,3 +170,80 @@ def test_plan_counts_and_residual_reduction_gloo():
         b0 = case.blocks[0]
         assert stats.max_loc == (0, 7 % b0.idim + 1, (7 // b0.idim) % b0.jdim + 1, 7 // (b0.idim * b0.jdim) + 1, 5)
         assert stats.phydtime == 0.01
+
+
+class _HostShard:
+    """Stands in for a Shard on the host: exchange sizes from a formula, pack
+    writes values naming sender, receiver, kind and position, unpack keeps
+    what arrived."""
+
+    def __init__(self, rank, nshards):
+        self.rank, self.nshards, self.device = rank, nshards, 0
+        self.got = {}
+
+    @staticmethod
+    def size(src, dst, kind):
+        return 3 + 2 * src + dst + 4 * kind
+
+    def counts(self, kind, peer):
+        return self.size(self.rank, peer, kind), self.size(peer, self.rank, kind)
+
+    @staticmethod
+    def values(src, dst, kind):
+        n = _HostShard.size(src, dst, kind)
+        return 1000.0 * src + 100.0 * dst + 10.0 * kind + np.arange(n)
+
+    def pack(self, kind, peer, ptr):
+        import ctypes
+        v = self.values(self.rank, peer, kind)
+        ctypes.memmove(ptr, v.ctypes.data, v.nbytes)
+
+    def unpack(self, kind, peer, ptr):
+        import ctypes
+        n = self.size(peer, self.rank, kind)
+        a = np.empty(n)
+        ctypes.memmove(a.ctypes.data, ptr, a.nbytes)
+        self.got[(kind, peer)] = a
+
+    def sync(self):
+        pass
+
+
+def _transport_main(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import datetime
+
+    import torch.distributed as dist
+
+    from orion_b200 import shard as sh
+    from test_shard_cpu import _HostShard
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    s = _HostShard(rank, world)
+    t = sh.DistTransport(buffer_device="cpu")
+    for _ in range(2):  # buffers are reused across exchanges
+        t.exchange([s], sh.HALO)
+        t.exchange([s], sh.IFACE)
+    q.put((rank, {k: v.tolist() for k, v in s.got.items()}))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_dist_transport_pairs_every_send_with_its_receive_gloo():
+    world = 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_transport_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = dict(q.get(timeout=180) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, got in out.items():
+        assert len(got) == 2 * (world - 1)
+        for (kind, peer), vals in got.items():
+            assert vals == _HostShard.values(peer, rank, kind).tolist()
