@@ -1382,7 +1382,7 @@ __device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
 
 template <typename S, typename T, int MODE, int NT>
-__global__ void __launch_bounds__(NT, 2) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
+__global__ void __launch_bounds__(NT, 512 / NT) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
                                                     const Chunk* __restrict__ chunks, ParamsDev P) {
   constexpr int Q0 = MODE == SW_LUSGS_BWD ? 3 : 0;
   constexpr int Q1 = MODE == SW_LUSGS_FWD ? 3 : 6;

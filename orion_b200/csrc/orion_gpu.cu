@@ -329,7 +329,7 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off, const Ex
       void* dnb = b64 ? (void*)b64->sk_nb : (void*)b32->sk_nb;
       CUDA_TRY(cudaMemcpyAsync(dnb, nbv.data(), nbv.size() * 4, cudaMemcpyHostToDevice, c->stream));
     }
-    // 256 points per sweep chunk (one per thread): more, smaller CTAs per hyperplane
+    // kSweepThreads points per sweep chunk, one per thread
     const int nt = kSweepThreads;
     L.sweep_nt = nt;
     for (int dir = 0; dir < 2; ++dir) {
