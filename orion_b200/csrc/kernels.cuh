@@ -1381,8 +1381,13 @@ __device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.w
 __device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
 
+// Threads per SM the per-hyperplane kernel is compiled for (register cap
+// 65536 / this): 512 measured fastest on the 64-block 385x257x129 case.
+#ifndef ORION_SWEEP_SM_THREADS
+#define ORION_SWEEP_SM_THREADS 512
+#endif
 template <typename S, typename T, int MODE, int NT>
-__global__ void __launch_bounds__(NT, 512 / NT) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
+__global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
                                                     const Chunk* __restrict__ chunks, ParamsDev P) {
   constexpr int Q0 = MODE == SW_LUSGS_BWD ? 3 : 0;
   constexpr int Q1 = MODE == SW_LUSGS_FWD ? 3 : 6;
