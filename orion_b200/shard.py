@@ -20,6 +20,10 @@ location identical, the rms equal up to the order of one sum.
 * DistTransport: one shard per process over torch.distributed point-to-point
   (NCCL between GPUs; the shard's buffers are CUDA tensors).
 * ShardGroup(shards, transport).step(): one step in OrionSolver::solve's order.
+
+    python -m orion_b200.shard --config 3 --shards 4 --precision mixed
+
+times a configuration as shards on one GPU against the same case as one.
 """
 from __future__ import annotations
 
@@ -315,3 +319,76 @@ class ShardGroup:
 
     def run(self, nsteps: int) -> List[ResidualStats]:
         return [self.step() for _ in range(nsteps)]
+
+
+def _per_stage_step(fs, nvis: int):
+    from . import solver
+    halo = solver.HaloExchanger()
+    halo.exchange_bc(None, fs)
+    solver.apply_physical_bc(None, fs)
+    solver.StateUpdater.update_flow_states(fs)
+    solver.TimeIntegrator.calculate_time_step(fs)
+    solver.FluxComputer.compute_viscous_rhs(fs)
+    if nvis == 1:
+        halo.average_interface_residuals(None, fs)
+    solver.InviscidFluxComputer.compute_inviscid_rhs(fs)
+    halo.average_interface_residuals(None, fs)
+    solver.StateUpdater.update_solution(fs)
+    return solver.ResidualMonitor.compute(fs)
+
+
+def main(argv=None):
+    """One GPU: a configuration as N shards (LocalTransport) against the same
+    case through the same per-stage entry points, wall clock per step (both
+    wait for the residual every step), and the bytes the shards exchange."""
+    import argparse
+    import json
+    import time
+
+    from . import cases, solver
+
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--config", type=int, default=3)
+    ap.add_argument("--shards", type=int, default=4)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=2)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "plain"])
+    a = ap.parse_args(argv)
+    case = cases.config(a.config)
+    prec = _lib.PREC_MIXED if a.precision == "mixed" else _lib.PREC_FP64
+    nvis = case.params.nvis
+
+    fs = solver.FlowFieldSet(case, precision=prec)
+    for _ in range(a.warmup):
+        _per_stage_step(fs, nvis)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        r1 = _per_stage_step(fs, nvis)
+    single = (time.perf_counter() - t0) / a.steps
+    fs.close()
+
+    owner = partition(case, a.shards)
+    shards = [Shard(case, owner, r, precision=prec) for r in range(a.shards)]
+    group = ShardGroup(shards, LocalTransport())
+    for _ in range(a.warmup):
+        group.step()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        r2 = group.step()
+    sharded = (time.perf_counter() - t0) / a.steps
+    halo = sum(s.counts(HALO, p.rank)[0] for s in shards for p in shards if p.rank != s.rank)
+    iface = sum(s.counts(IFACE, p.rank)[0] for s in shards for p in shards if p.rank != s.rank)
+    for s in shards:
+        s.close()
+    print(json.dumps({
+        "workload": case.name, "precision": a.precision, "shards": a.shards, "owner": owner,
+        "steps": a.steps, "ms_per_step_single_per_stage": single * 1e3, "ms_per_step_sharded": sharded * 1e3,
+        "exchanged_bytes_per_step": 8 * (halo + (2 if nvis == 1 else 1) * iface),
+        "halo_bytes": 8 * halo, "iface_bytes_per_average": 8 * iface,
+        "same_residual_max": r1.max_residual == r2.max_residual and tuple(r1.max_loc) == tuple(r2.max_loc),
+        "timing": "wall clock; both paths wait for the residual every step, the sharded one also at every exchange",
+    }))
+
+
+if __name__ == "__main__":
+    main()
