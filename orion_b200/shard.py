@@ -224,51 +224,70 @@ class DistTransport:
     """One shard per process over torch.distributed point-to-point: every rank
     posts its sends and receives to every peer together (batch_isend_irecv),
     so the order of ranks cannot deadlock.  The packs finish before the
-    transfer starts and the transfer before the unpacks.  Buffers live on the
-    shard's GPU (NCCL); `buffer_device="cpu"` keeps them in host memory for a
-    gloo group."""
+    transfer starts and the transfer before the unpacks.
 
-    def __init__(self, group=None, buffer_device=None):
+    * Default: the buffers live on the shard's GPU and the group moves them
+      (NCCL between GPUs).
+    * host_staging=True: the shard packs into and unpacks from its GPU
+      buffers, and host copies of them cross the group (gloo over TCP, for
+      machines without a GPU-to-GPU path).
+    * buffer_device="cpu": the buffers themselves are host memory; only for
+      shards whose pack/unpack work on host memory."""
+
+    def __init__(self, group=None, buffer_device=None, host_staging: bool = False):
         import torch.distributed as dist
         self.dist = dist
         self.group = group
         self.buffer_device = buffer_device
+        self.host_staging = host_staging
         self._bufs: Dict[Tuple[int, int, str], object] = {}
 
-    def _buf(self, kind: int, peer: int, side: str, n: int, device: int):
-        key = (kind, peer, side)
+    def _buf(self, kind: int, peer: int, side: str, n: int, device):
+        key = (kind, peer, side, str(device))
         b = self._bufs.get(key)
         if b is None or b.numel() < n:
-            b = self._bufs[key] = _device_buffer(n, self.buffer_device or device)
+            b = self._bufs[key] = _device_buffer(n, device)
         return b
 
     def exchange(self, shards: Sequence[Shard], kind: int):
         import torch
         (s,) = shards
-        ops, recvs = [], []
+        dev = self.buffer_device or s.device
+        ops, sends, recvs = [], [], []
         for peer in range(s.nshards):
             if peer == s.rank:
                 continue
             nsend, nrecv = s.counts(kind, peer)
             if nsend:
-                b = self._buf(kind, peer, "send", nsend, s.device)
+                b = self._buf(kind, peer, "send", nsend, dev)
                 s.pack(kind, peer, b.data_ptr())
-                ops.append(self.dist.P2POp(self.dist.isend, b[:nsend], peer, self.group))
+                sends.append((peer, b[:nsend]))
             if nrecv:
-                b = self._buf(kind, peer, "recv", nrecv, s.device)
-                ops.append(self.dist.P2POp(self.dist.irecv, b[:nrecv], peer, self.group))
-                recvs.append((peer, b))
-        s.sync()
+                recvs.append((peer, self._buf(kind, peer, "recv", nrecv, dev)[:nrecv]))
+        s.sync()  # packs done before anything reads the buffers
+        for peer, b in sends:
+            w = self._buf(kind, peer, "send-host", b.numel(), "cpu")[:b.numel()] if self.host_staging else b
+            if self.host_staging:
+                w.copy_(b)
+            ops.append(self.dist.P2POp(self.dist.isend, w, peer, self.group))
+        wires = []
+        for peer, b in recvs:
+            w = self._buf(kind, peer, "recv-host", b.numel(), "cpu")[:b.numel()] if self.host_staging else b
+            wires.append(w)
+            ops.append(self.dist.P2POp(self.dist.irecv, w, peer, self.group))
         if ops:
             for req in self.dist.batch_isend_irecv(ops):
                 req.wait()
+        if self.host_staging:
+            for (peer, b), w in zip(recvs, wires):
+                b.copy_(w)
         if self.buffer_device is None:
-            torch.cuda.synchronize(s.device)
+            torch.cuda.synchronize(s.device)  # received data in place before the case's stream reads it
         for peer, b in recvs:
             s.unpack(kind, peer, b.data_ptr())
 
     def reduce(self, shards: Sequence[Shard], parts) -> List[Tuple[float, float, int, float]]:
-        dev = self.buffer_device or f"cuda:{shards[0].device}"
+        dev = "cpu" if (self.host_staging or self.buffer_device) else f"cuda:{shards[0].device}"
         return gather_partials(parts[0], self.dist, self.group, device=dev)
 
 

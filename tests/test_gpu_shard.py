@@ -93,3 +93,63 @@ def test_shard_refuses_whole_case_calls():
     send, recv = s.counts(shard.HALO, 1)
     assert send > 0 and recv > 0
     s.close()
+
+
+def _free_port():
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _dist_rank(rank, world, port, q):
+    """One shard per process on the same GPU, exchanges staged through host
+    memory over gloo: no kernel of one process waits for another's."""
+    import datetime
+    import os
+    import sys
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import torch.distributed as dist
+
+    from orion_b200 import _lib as L
+    from orion_b200 import cases as cs
+    from orion_b200 import shard as sh
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    case = cs.small_case("sh", dims=(61, 45, 37), split=(3, 2, 2), uneven_seed=5, noise_seed=3)
+    s = sh.Shard(case, sh.partition(case, world), rank, precision=L.PREC_FP64)
+    stats = sh.ShardGroup([s], sh.DistTransport(host_staging=True)).run(3)
+    prim = {g: s.download(g, "prim") for g in s.global_ids}
+    s.close()
+    q.put((rank, [(t.rms_residual, t.max_residual, tuple(t.max_loc), t.phydtime) for t in stats], prim))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_one_shard_per_process_host_staged_equals_single_case():
+    import torch.multiprocessing as mp
+
+    case = cases.small_case("sh", dims=(61, 45, 37), split=(3, 2, 2), uneven_seed=5, noise_seed=3)
+    hist, prim1 = _single(case, _lib.PREC_FP64, 3)
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_dist_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    prim = [None] * len(case.blocks)
+    for rank, stats, blocks in out:
+        for (rms, mx, loc, dt), h in zip(stats, hist):
+            assert mx == h.max_residual and loc == tuple(h.max_loc) and dt == h.phydtime
+            assert abs(rms - h.rms_residual) <= 1e-12 * h.rms_residual
+        for g, a in blocks.items():
+            prim[g] = a
+    for b, (a, c) in enumerate(zip(prim1, prim)):
+        assert c is not None and np.array_equal(a, c), f"block {b}"
