@@ -27,7 +27,7 @@ from __future__ import annotations
 import math
 import os
 from dataclasses import dataclass, field
-from typing import List, Optional, Sequence, Tuple
+from typing import Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -225,9 +225,12 @@ def uneven_splits(n: int, parts: int, rng: np.random.Generator, ratio: float = 3
 
 def split_case(name: str, x: np.ndarray, y: np.ndarray, z: np.ndarray,
                si: Sequence[int], sj: Sequence[int], sk: Sequence[int],
-               params: FlowParams, nsteps: int, noise_seed: int, noise_amp: float = 0.01) -> Case:
+               params: FlowParams, nsteps: int, noise_seed: int, noise_amp: float = 0.01,
+               physical: Optional[Dict[str, int]] = None) -> Case:
     """Cut a global grid into blocks at the given shared planes and build the
-    region lists (physical BCs on the domain boundary, interfaces inside)."""
+    region lists (physical BCs on the domain boundary, interfaces inside).
+    `physical` overrides the BC type of domain faces (PHYSICAL_TYPE)."""
+    types = {**PHYSICAL_TYPE, **(physical or {})}
     nbi, nbj, nbk = len(si) - 1, len(sj) - 1, len(sk) - 1
     blocks: List[Block] = []
 
@@ -256,7 +259,7 @@ def split_case(name: str, x: np.ndarray, y: np.ndarray, z: np.ndarray,
                     s_st, s_ed = face_window(blk.dims, f)
                     nb = neighbour(a, b, c, f, nbi, nbj, nbk)
                     if nb is None:
-                        blk.regions.append(Region(s_st, s_ed, PHYSICAL_TYPE[f]))
+                        blk.regions.append(Region(s_st, s_ed, types[f]))
                     else:
                         tgt = blocks[bid(*nb)]
                         t_st, t_ed = face_window(tgt.dims, OPPOSITE[f])
@@ -296,15 +299,20 @@ def neighbour(a, b, c, face, nbi, nbj, nbk):
 def bump_case(name: str, NI: int, NJ: int, NK: int, *, height: float = 0.05,
               split: Tuple[int, int, int] = (1, 1, 1), uneven_seed: Optional[int] = None,
               moo: float = 0.5, reynolds: float = 1000.0, nsteps: int = 1,
-              noise_seed: int = 0, noise_amp: float = 0.01, cfl: float = 2.0) -> Case:
+              noise_seed: int = 0, noise_amp: float = 0.01, cfl: float = 2.0,
+              physical: Optional[Dict[str, int]] = None, nvis: int = 1, twall: float = 0.0,
+              attack: float = 0.0, method: int = 1) -> Case:
+    """A bump channel split into blocks.  physical: BC type per domain face
+    (default PHYSICAL_TYPE); nvis 0 = Euler; twall > 0 = isothermal walls;
+    attack in degrees; method 0 skips the wall-normal averaging."""
     x, y, z = bump_grid(NI, NJ, NK, height)
     if uneven_seed is None:
         si, sj, sk = (even_splits(n, p) for n, p in zip((NI, NJ, NK), split))
     else:
         rng = np.random.default_rng(uneven_seed)
         si, sj, sk = (uneven_splits(n, p, rng) for n, p in zip((NI, NJ, NK), split))
-    params = FlowParams(moo=moo, reynolds=reynolds, cfl=cfl)
-    return split_case(name, x, y, z, si, sj, sk, params, nsteps, noise_seed, noise_amp)
+    params = FlowParams(moo=moo, reynolds=reynolds, cfl=cfl, nvis=nvis, twall=twall, attack=attack, method=method)
+    return split_case(name, x, y, z, si, sj, sk, params, nsteps, noise_seed, noise_amp, physical=physical)
 
 
 def config(n: int, nsteps: Optional[int] = None) -> Case:
@@ -330,10 +338,11 @@ def config(n: int, nsteps: Optional[int] = None) -> Case:
 
 def small_case(name: str = "small", dims=(25, 17, 13), split=(1, 1, 1), nsteps: int = 3,
                moo: float = 0.5, reynolds: float = 1000.0, noise_seed: int = 7,
-               uneven_seed: Optional[int] = None, height: float = 0.05) -> Case:
-    """A case small enough for the CPU oracle to step in well under a second."""
+               uneven_seed: Optional[int] = None, height: float = 0.05, **flow) -> Case:
+    """A case small enough for the CPU oracle to step in well under a second.
+    `flow`: the optional bump_case settings (physical, nvis, twall, attack, method)."""
     return bump_case(name, *dims, height=height, split=split, uneven_seed=uneven_seed, moo=moo,
-                     reynolds=reynolds, nsteps=nsteps, noise_seed=noise_seed)
+                     reynolds=reynolds, nsteps=nsteps, noise_seed=noise_seed, **flow)
 
 
 # ---------------------------------------------------------------------------

@@ -6,7 +6,8 @@
   device pow by an ulp: tolerance 1e-13 relative there);
 * whole runs: residual history and final state against the committed golden
   fixtures and, when oracle/_ref is present, against live reference runs of
-  multi-block cases, within 1e-10 relative.
+  multi-block cases and of cases with freestream, extrapolation and
+  isothermal-wall BCs and an Euler case, within 1e-10 relative.
 """
 import json
 import os
@@ -43,6 +44,12 @@ STAGE_CASES = {
     "multi8": dict(name="multi8", dims=(33, 25, 23), split=(2, 2, 2), noise_seed=8),
     "uneven_transonic": dict(name="uneven", dims=(41, 27, 25), split=(3, 2, 2), noise_seed=9, uneven_seed=4,
                              moo=0.8, reynolds=1.0e5, height=0.08),
+    # freestream and extrapolation faces, isothermal walls, flow at 3 degrees of attack
+    "bc_mix": dict(name="bcmix", dims=(33, 25, 23), split=(2, 1, 1), noise_seed=10, twall=300.0, attack=3.0,
+                   physical={"imin": cases.BC_FREESTREAM, "imax": cases.BC_EXTRAPOLATION,
+                             "kmax": cases.BC_EXTRAPOLATION}),
+    # Euler: slip walls, no viscous stage; method 0 (no wall-normal averaging)
+    "inviscid_m0": dict(name="inviscid", dims=(33, 25, 23), split=(1, 2, 1), noise_seed=11, nvis=0, method=0),
 }
 
 
@@ -51,12 +58,16 @@ STAGE_CASES = {
 def test_stage_parity(key, tmp_path):
     case = cases.small_case(nsteps=2, **STAGE_CASES[key])
     _, odir = run_reference_case(case, 2, snap_step=1, workdir=str(tmp_path))
-    snaps = {s: refio.read_state(os.path.join(odir, f"snap_1_{s}.bin")) for s in STAGES}
+    # without viscosity the reference runs neither the viscous stage nor its averaging
+    skip = set() if case.params.nvis == 1 else {"visc", "avg1"}
+    snaps = {s: refio.read_state(os.path.join(odir, f"snap_1_{s}.bin")) for s in STAGES if s not in skip}
     hist = refio.read_hist(os.path.join(odir, "hist.bin"))
     pre = snaps["pre"]
     fs = solver.FlowFieldSet(case, init=False, metrics=[(b["metrics"], b["vol"]) for b in pre["blocks"]])
     prev = "pre"
     for name, fn, fields, tol in _stage_ops(fs):
+        if name in skip:
+            continue
         fs.upload_state(snaps[prev])
         fn()
         fs.sync()
@@ -93,6 +104,24 @@ def test_whole_run_matches_golden(key):
     prim = np.concatenate([fs.download(b, "prim")[:5, 3:-3, 3:-3, 3:-3].reshape(5, -1)
                            for b in range(len(case.blocks))], axis=1)[:, ::sub]
     assert rel_err(prim, g["prim"]) <= TOL_RUN
+    fs.close()
+
+
+@needs_ref
+@pytest.mark.parametrize("key", ["bc_mix", "inviscid_m0"])
+def test_whole_run_matches_reference_other_bcs(key, tmp_path):
+    """Five steps of the cases with the other BC types and flow options, against live reference runs."""
+    case = cases.small_case(nsteps=5, **STAGE_CASES[key])
+    _, odir = run_reference_case(case, 5, workdir=str(tmp_path))
+    ref_hist = refio.read_hist(os.path.join(odir, "hist.bin"))
+    ref = refio.read_state(os.path.join(odir, "final.bin"))
+    fs = solver.FlowFieldSet(case)
+    hist = fs.step(5)
+    for col in (0, 1, 7):
+        assert np.max(np.abs(hist[:, col] - ref_hist[:, col]) / np.abs(ref_hist[:, col])) <= TOL_RUN, col
+    assert np.array_equal(hist[:, 2:7], ref_hist[:, 2:7])
+    for n, blk in enumerate(ref["blocks"]):
+        assert rel_err(interior(fs.download(n, "prim")[:5]), interior(blk["prim"][:5])) <= TOL_RUN
     fs.close()
 
 
