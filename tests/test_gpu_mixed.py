@@ -60,6 +60,23 @@ def test_mixed_tracks_fp64_on_uneven_multiblock_case():
     fp.close()
 
 
+@pytest.mark.parametrize("name,flow", [
+    ("mixedbc", dict(twall=300.0, attack=3.0, physical={"imin": cases.BC_FREESTREAM, "imax": cases.BC_EXTRAPOLATION,
+                                                         "kmax": cases.BC_EXTRAPOLATION})),
+    ("mixedeuler", dict(nvis=0, method=0)),
+])
+def test_mixed_tracks_fp64_with_other_bcs_and_euler(name, flow):
+    """Freestream / extrapolation faces, isothermal walls and attack; and the
+    Euler path (slip walls, no viscous stage)."""
+    case = cases.small_case(name, dims=(33, 25, 23), split=(2, 1, 1), noise_seed=12, **flow)
+    fm, fp = _pair(case)
+    fm.step(10)
+    fp.step(10)
+    assert _rel_l2(case, fm, fp) <= TOL_L2
+    fm.close()
+    fp.close()
+
+
 def test_mixed_path_stores_increments_in_fp32():
     case = cases.small_case("mixedfp", dims=(25, 17, 13))
     fm, fp = _pair(case)
