@@ -2,12 +2,12 @@
 solver (compiled from its own sources into oracle/_ref by oracle/Makefile) on
 small seeded cases.
 
-    make -C oracle ref && python tests/golden/gen_golden.py
+    make -C oracle ref && python tests/golden/gen_golden.py [fixture ...]
 
 Each fixture holds the case recipe, the reference's residual history
 (rms, max, max location, phydtime per step) and its final primitive state:
-the full interior state for the single-block case, every 7th interior point
-(flattened, blocks in order) for the multi-block case to keep the file small.
+the full interior state for a single-block case, every 7th interior point
+(flattened, blocks in order) for a multi-block case to keep the file small.
 """
 from __future__ import annotations
 
@@ -33,6 +33,13 @@ RECIPES = {
     "small_8blk": dict(name="small_8blk", dims=(33, 25, 23), split=(2, 2, 2), nsteps=10, noise_seed=12),
     "small_uneven": dict(name="small_uneven", dims=(41, 27, 25), split=(3, 2, 2), nsteps=8, noise_seed=13,
                          uneven_seed=5, moo=0.7, reynolds=1.0e4),
+    # freestream (imin) and extrapolation (imax, kmax) faces, isothermal walls, 3 degrees of attack
+    "small_bcmix": dict(name="small_bcmix", dims=(33, 25, 23), split=(2, 1, 1), nsteps=8, noise_seed=14,
+                        twall=300.0, attack=3.0, physical={"imin": cases.BC_FREESTREAM, "imax": cases.BC_EXTRAPOLATION,
+                                                           "kmax": cases.BC_EXTRAPOLATION}),
+    # Euler: slip walls, no viscous stage; method 0
+    "small_euler": dict(name="small_euler", dims=(33, 25, 23), split=(1, 2, 1), nsteps=8, noise_seed=15,
+                        nvis=0, method=0),
 }
 
 
@@ -50,8 +57,10 @@ def interior_prim(state, sub: int = 1) -> np.ndarray:
     return flat[:, ::sub]
 
 
-def main():
+def main(keys=None):
     for key, recipe in RECIPES.items():
+        if keys and key not in keys:
+            continue
         case = build(recipe)
         tmp = tempfile.mkdtemp(prefix="golden_")
         case.write_reference_inputs(os.path.join(tmp, "case"))
@@ -65,4 +74,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

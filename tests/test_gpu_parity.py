@@ -89,7 +89,7 @@ def test_stage_parity(key, tmp_path):
     fs.close()
 
 
-@pytest.mark.parametrize("key", ["small_1blk", "small_8blk", "small_uneven"])
+@pytest.mark.parametrize("key", ["small_1blk", "small_8blk", "small_uneven", "small_bcmix", "small_euler"])
 def test_whole_run_matches_golden(key):
     g = np.load(os.path.join(ROOT, "tests", "golden", key + ".npz"))
     case = cases.small_case(**json.loads(str(g["recipe"][0])))

@@ -140,7 +140,7 @@ def test_metrics_unit_cube_volume():
 
 
 @needs_ref
-@pytest.mark.parametrize("key", ["small_1blk", "small_8blk"])
+@pytest.mark.parametrize("key", ["small_1blk", "small_8blk", "small_bcmix", "small_euler"])
 def test_golden_fixtures_reproduce(key, tmp_path):
     """The committed golden fixtures are what the reference produces today."""
     import sys
@@ -159,7 +159,7 @@ def test_golden_fixtures_reproduce(key, tmp_path):
 
 
 def test_golden_fixture_recipes_load():
-    for f in ("small_1blk", "small_8blk", "small_uneven"):
+    for f in ("small_1blk", "small_8blk", "small_uneven", "small_bcmix", "small_euler"):
         g = np.load(os.path.join(ROOT, "tests", "golden", f + ".npz"))
         recipe = json.loads(str(g["recipe"][0]))
         c = cases.small_case(**recipe)
