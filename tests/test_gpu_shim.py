@@ -25,6 +25,10 @@ CASES = {
     "multi8": dict(name="multi8", dims=(33, 25, 23), split=(2, 2, 2), noise_seed=8),
     "uneven_transonic": dict(name="uneven", dims=(41, 27, 25), split=(3, 2, 2), noise_seed=9, uneven_seed=4,
                              moo=0.8, reynolds=1.0e5, height=0.08),
+    "bc_mix": dict(name="bcmix", dims=(33, 25, 23), split=(2, 1, 1), noise_seed=10, twall=300.0, attack=3.0,
+                   physical={"imin": cases.BC_FREESTREAM, "imax": cases.BC_EXTRAPOLATION,
+                             "kmax": cases.BC_EXTRAPOLATION}),
+    "euler": dict(name="euler", dims=(33, 25, 23), split=(1, 2, 1), noise_seed=11, nvis=0, method=0),
 }
 NSTEPS = 5
 
@@ -42,7 +46,8 @@ def _runs(key, tmp_path, extra):
 
 @needs
 @pytest.mark.parametrize("key,mode", [("multi8", "coherent"), ("multi8", "resident"),
-                                      ("uneven_transonic", "coherent")])
+                                      ("uneven_transonic", "coherent"), ("bc_mix", "coherent"),
+                                      ("euler", "resident")])
 def test_reference_driver_on_device_matches_reference(key, mode, tmp_path):
     (href, sref), (hgpu, sgpu) = _runs(key, tmp_path, ["--resident"] if mode == "resident" else [])
     assert np.all(np.abs(hgpu[:, :2] - href[:, :2]) <= TOL_RUN * np.abs(href[:, :2]))
