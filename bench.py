@@ -67,7 +67,7 @@ def hbm_peak():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             return float(json.load(f)["hbm_gbs"]), "measured"
-    except Exception:
+    except (OSError, KeyError, TypeError, ValueError):
         return FALLBACK_HBM_GBS, "fallback"
 
 
@@ -91,7 +91,7 @@ class Clocks:
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
-        except Exception:
+        except OSError:  # no nvidia-smi: the line says "unsampled"
             self.proc = None
 
     def _read(self):
@@ -104,7 +104,7 @@ class Clocks:
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
-        except Exception:
+        except subprocess.TimeoutExpired:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
