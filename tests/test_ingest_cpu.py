@@ -29,6 +29,22 @@ def test_written_case_reads_back(tmp_path, split, seed):
         assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y) and np.array_equal(a.z, b.z)
 
 
+def test_other_bc_types_and_flow_options_read_back(tmp_path):
+    """Freestream / extrapolation faces, isothermal walls, attack, Euler and
+    method 0 survive the reference's file formats."""
+    c = cases.small_case("opts", dims=(33, 25, 23), split=(2, 1, 1), nsteps=4, noise_seed=3, twall=300.0,
+                         attack=3.0, nvis=0, method=0,
+                         physical={"imin": cases.BC_FREESTREAM, "imax": cases.BC_EXTRAPOLATION})
+    types = {r.bctype for b in c.blocks for r in b.regions}
+    assert {cases.BC_FREESTREAM, cases.BC_EXTRAPOLATION, cases.BC_WALL, cases.BC_INTERFACE} <= types
+    c.write_reference_inputs(str(tmp_path))
+    r = cases.read_case(str(tmp_path))
+    assert r.params == c.params
+    assert (r.params.nvis, r.params.method, r.params.twall, r.params.attack) == (0, 0, 300.0, 3.0)
+    for a, b in zip(r.blocks, c.blocks):
+        assert a.regions == b.regions
+
+
 def test_unsupported_and_malformed_inputs_are_rejected(tmp_path):
     c = cases.small_case("bad", dims=(25, 17, 13))
     c.write_reference_inputs(str(tmp_path))
