@@ -247,3 +247,50 @@ def test_dist_transport_pairs_every_send_with_its_receive_gloo():
         assert len(got) == 2 * (world - 1)
         for (kind, peer), vals in got.items():
             assert vals == _HostShard.values(peer, rank, kind).tolist()
+
+
+def _dead_peer_main(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import datetime
+    import time
+
+    import torch.distributed as dist
+
+    from orion_b200 import shard as sh
+    from test_shard_cpu import _HostShard
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    dist.barrier()
+    if rank == 1:  # this rank leaves between steps, before the next exchange
+        q.put((1, "left"))
+        q.close()
+        q.join_thread()
+        os._exit(0)
+    t0 = time.time()
+    try:
+        sh.DistTransport(buffer_device="cpu").exchange([_HostShard(0, world)], sh.HALO)
+        msg = "no error"
+    except Exception as e:  # the survivor learns of it on the host
+        msg = f"raised {type(e).__name__} after {time.time() - t0:.1f} s"
+    q.put((0, msg))
+    q.close()
+    q.join_thread()
+    os._exit(0)
+
+
+def test_exchange_with_a_departed_rank_fails_on_the_host_gloo():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_dead_peer_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = dict(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+    assert out[1] == "left"
+    assert out[0].startswith("raised"), out[0]
+    assert float(out[0].split()[-2]) < 60.0
