@@ -1,10 +1,10 @@
 """Block sharding, host side (no GPU).
 
 * The exchange plan (orion_b200/csrc/exchange_plan.hpp) compiled on the host:
-  for several owner maps per case, exchange_bc and the interface averaging
-  done shard by shard with explicit pack -> wire -> unpack equal, bit for bit
-  on every block, the same exchanges done with the single-case lists
-  (tests/shard/plan_check.cpp).
+  for several owner maps per case (fixed layouts, then seeded random splits
+  and maps), exchange_bc and the interface averaging done shard by shard with
+  explicit pack -> wire -> unpack equal, bit for bit on every block, the same
+  exchanges done with the single-case lists (tests/shard/plan_check.cpp).
 * The library's host-only plan counts agree between the two ends of every
   pair when each rank computes its own (gloo, world size 2).
 * The residual reduction over ranks (gloo) equals the single-case reduction
@@ -294,3 +294,33 @@ def test_exchange_with_a_departed_rank_fails_on_the_host_gloo():
     assert out[1] == "left"
     assert out[0].startswith("raised"), out[0]
     assert float(out[0].split()[-2]) < 60.0
+
+
+def test_sharded_exchanges_equal_single_case_random_layouts(plan_check):
+    """Seeded random splits (even and uneven, up to 3 x 3 x 2 blocks) and owner
+    maps (up to 4 shards): the sharded exchanges equal the single-case ones."""
+    rng = np.random.default_rng(2024)
+    for trial in range(6):
+        split = tuple(int(v) for v in (rng.integers(1, 4), rng.integers(1, 4), rng.integers(1, 3)))
+        if split == (1, 1, 1):
+            split = (2, 1, 1)
+        dims = tuple(int(13 * s + rng.integers(0, 9)) for s in split)
+        uneven = int(rng.integers(0, 100)) if trial % 2 else None
+        try:
+            case = cases.small_case(f"r{trial}", dims=dims, split=split, uneven_seed=uneven)
+        except ValueError:  # an uneven cut below the minimum block extent
+            case = cases.small_case(f"r{trial}", dims=dims, split=split)
+        nb = len(case.blocks)
+        maps = []
+        for _ in range(3):
+            k = int(rng.integers(2, min(4, nb) + 1))
+            m = [int(v) for v in rng.integers(0, k, nb)]
+            ids = {v: i for i, v in enumerate(sorted(set(m)))}
+            m = [ids[v] for v in m]
+            if max(m) >= 1:
+                maps.append(m)
+        if not maps:
+            continue
+        r = subprocess.run([plan_check], input=_describe(case, maps), capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, (split, dims, r.stdout + r.stderr)
+        assert sum("identical" in ln for ln in r.stdout.splitlines()) == len(maps)
