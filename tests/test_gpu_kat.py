@@ -13,16 +13,17 @@ states whose result is known in closed form, independent of the oracle.
   Sutherland mu, Q.
 5 time step (:387-494): metrics diag 10, vol 1e-3, rho = p = 1, mu = 0.1,
   Re = 1000, cfl = 1: dt = cfl / (3 (c 10 + 2 mu 100 / (Re rho vol))) / vol.
+6 viscous exactness (:499-593): u = y^2, metrics diag 0.01, vol 1e-3,
+  mu = 0.1, Re = 1000: dq(x-momentum) at the block centre = -2.0e-7.
 7 interface averaging (:598-677): vol = 1, dq = block id + 1000; the
   interface face centre holds the mean of the two blocks.
-(6, the viscous-flux exactness check, is covered by the stage parity tests.)
 """
 import math
 
 import numpy as np
 import pytest
 
-from orion_b200 import _lib, cases, solver
+from orion_b200 import cases, solver
 
 pytestmark = pytest.mark.gpu
 NG = cases.NG
@@ -154,6 +155,34 @@ def test_kat5_time_step():
     dt = fs.download(0, "dt")[NG:-NG, NG:-NG, NG:-NG]
     assert np.allclose(dt, dt_phys / 1e-3, rtol=1e-13, atol=0)
     assert phydtime == pytest.approx(dt_phys, rel=1e-13)
+    fs.close()
+
+
+def test_kat6_viscous_exactness():
+    """u = y^2 on the grid that metrics diag 0.01 and vol 1e-3 describe (spacing
+    0.1): tau_xy = 2 mu y, its eta-face flux 0.01 tau_xy differences to
+    2e-4 per index, so dq(x-momentum) = -2e-4 / Re = -2e-7.  The stencils are
+    exact on a quadratic; the xi and zeta fluxes of x-momentum vanish."""
+    case = cases.small_case("kat6", dims=(25, 25, 25), reynolds=1000.0)
+    b = case.blocks[0]
+    nx, ny, nz = b.padded
+    fs = solver.FlowFieldSet(case)
+    met = np.zeros((9, nz, ny, nx))
+    met[0] = met[4] = met[8] = 0.01
+    fs.upload(0, "metrics", met)
+    fs.upload(0, "vol", np.full((nz, ny, nx), 1e-3))
+    _, j, _ = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    prim = np.zeros((6, nz, ny, nx))
+    prim[0] = prim[4] = prim[5] = 1.0
+    prim[1] = (0.1 * (j - NG)) ** 2
+    fs.upload(0, "prim", prim)
+    fs.upload(0, "mu", np.full((nz, ny, nx), 0.1))
+    fs.upload(0, "dq", np.zeros((5, nz, ny, nx)))
+    solver.FluxComputer.compute_viscous_rhs(fs)
+    ic, jc, kc = _centre(b)
+    got = fs.download(0, "dq")[1, kc, jc, ic]
+    assert abs(got - (-2.0e-7)) <= 1e-10
+    assert got == pytest.approx(-2.0e-7, rel=1e-8)
     fs.close()
 
 
