@@ -121,12 +121,32 @@ inline std::string build_exchange_plan(const std::vector<HostBlock>& g, const st
         queue.push_back(std::move(msg));
       }
     }
+    {  // room for the pairs inside the shard: every owned ghost window, once
+      size_t est = 0;
+      for (int b = 0; b < nb; ++b) {
+        if (owner[b] != rank) continue;
+        const int dims[3] = {g[b].idim, g[b].jdim, g[b].kdim};
+        for (const auto& hr : g[b].regions) {
+          if (hr.r.nbt <= 0) continue;
+          int beg[3], end[3];
+          memory_window(hr, ng, dims, 1, beg, end);
+          size_t n = 5;
+          for (int d = 0; d < 3; ++d) n *= (size_t)std::max(0, end[d] - beg[d] + 1);
+          est += n;
+        }
+      }
+      p.halo_dst.reserve(est);
+      p.halo_src.reserve(est);
+    }
     std::vector<int> slot;
+    std::vector<long long> dst, src_el;  // per receiving block, reused
+    std::vector<int> src_blk;            // global block of each source element
     for (int b = 0; b < nb; ++b) {
       const auto& h = g[b];
       const int dims[3] = {h.idim, h.jdim, h.kdim};
-      std::vector<long long> dst;
-      std::vector<std::pair<int, long long>> src;  // global block, element
+      dst.clear();
+      src_el.clear();
+      src_blk.clear();
       if (concerns[b]) slot.assign((size_t)5 * h.npad, -1);
       for (int r = 0; r < (int)h.regions.size(); ++r) {
         const auto& hr = h.regions[r];
@@ -148,23 +168,26 @@ inline std::string build_exchange_plan(const std::vector<HostBlock>& g, const st
             if (sl < 0) {
               sl = (int)dst.size();
               dst.push_back(el);
-              src.emplace_back(it->sb, it->src[q]);
+              src_blk.push_back(it->sb);
+              src_el.push_back(it->src[q]);
             } else {
-              src[(size_t)sl] = {it->sb, it->src[q]};
+              src_blk[(size_t)sl] = it->sb;
+              src_el[(size_t)sl] = it->src[q];
             }
           }
         }
         queue.erase(it);
       }
+      const int ob = owner[b];
       for (size_t e = 0; e < dst.size(); ++e) {
-        const int sb = src[e].first, ob = owner[b], os = owner[sb];
+        const int sb = src_blk[e], os = owner[sb];
         if (ob == rank && os == rank) {
           p.halo_dst.push_back({p.local_of[b], dst[e]});
-          p.halo_src.push_back({p.local_of[sb], src[e].second});
+          p.halo_src.push_back({p.local_of[sb], src_el[e]});
         } else if (ob == rank) {
           p.halo_recv[os].push_back({p.local_of[b], dst[e]});
         } else if (os == rank) {
-          p.halo_send[ob].push_back({p.local_of[sb], src[e].second});
+          p.halo_send[ob].push_back({p.local_of[sb], src_el[e]});
         }
       }
     }
