@@ -241,15 +241,20 @@ int orion_case_poll(orion_case_t c, orion_residual_t* out, int cap, int* n);
  * where they need the residual (a solver that reserves its whole device budget
  * up front, a loop inside another framework's memory pool, a step that must not
  * let an allocation synchronize the device): computes the statistics of
- * orion_residual_compute for ONE block from device pointers the caller owns
- * (dq: 5 comps, vol, dt: padded layout, FP64) and writes them to the host
+ * orion_residual_compute for ONE block (rms, max and its location; phydtime
+ * is written as 0, since in the case-based path it is the time-step stage's
+ * dt minimum, which this call does not run) from device pointers the caller
+ * owns (dq: 5 comps, vol, dt: padded layout, FP64) and writes them to the host
  * struct `out`, waiting for `stream` (a cudaStream_t as void*, NULL = default).
  * Its scratch is a fixed array in the library's device memory, so blocks are
  * limited to ORION_NOALLOC_MAX_POINTS interior points (larger ones get
- * ORION_E_INVALID).  The first call on each device looks up that array's device
- * address; make it before any stream capture.  All calls on a device share the
- * array: calls that overlap on the GPU (different streams, or threads without
- * ordering) race and must not be issued. */
+ * ORION_E_INVALID).  Every call looks up that array's address in the current
+ * context; the first call on a device may load the library's device code, so
+ * make it before any stream capture on that device.  The call synchronizes
+ * `stream`, so it never runs on a capturing stream: it returns ORION_E_INVALID
+ * there.  All calls on a device share the array: calls that overlap on the GPU
+ * (different streams, or threads without ordering) race and must not be
+ * issued. */
 #define ORION_NOALLOC_MAX_POINTS 8388608
 int orion_residual_block_noalloc(const double* dq, const double* vol, const double* dt, int idim, int jdim,
                                  int kdim, void* stream, orion_residual_t* out);

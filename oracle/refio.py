@@ -19,8 +19,23 @@ FIELDS = (("prim", 6), ("q", 5), ("dq", 5), ("metrics", 9), ("vol", 1), ("dt", 1
           ("c", 1), ("mu", 1), ("spec", 3), ("specv", 3))
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-# The reference's source tree (read-only); only CPU-side checks read it directly.
-REF_ROOT = os.environ.get("ORION_REF", "/root/reference")
+
+
+def ref_root() -> str:
+    """The reference's source tree (read-only): $ORION_REF, else the default
+    that oracle/Makefile (the recipe compiling it) names.  Only CPU-side checks
+    read it directly; the GPU box has no source tree."""
+    env = os.environ.get("ORION_REF")
+    if env:
+        return env
+    with open(os.path.join(HERE, "Makefile")) as f:
+        for line in f:
+            if line.startswith("ORION_REF") and "?=" in line:
+                return line.split("?=", 1)[1].strip()
+    return ""
+
+
+REF_ROOT = ref_root()
 REF_HARNESS = os.path.join(HERE, "_ref", "orion_ref_harness")
 # The same driver source linked against the B200 path through the C++ drop-in
 # layer (make -C oracle shim); it is the product under test, not the oracle.

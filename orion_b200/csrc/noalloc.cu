@@ -11,7 +11,6 @@
 // memory, which every GPU that loads the library holds until the process exits.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "kernels.cuh"
@@ -101,9 +100,6 @@ __global__ void __launch_bounds__(1024) k_noalloc_final(NoAllocScratch* __restri
   }
 }
 
-std::mutex g_na_mutex;
-NoAllocScratch* g_na_ptr[64] = {nullptr};
-
 int na_fail(int code, const std::string& msg) { return orion::set_error(code, msg); }
 
 }  // namespace
@@ -116,21 +112,25 @@ extern "C" int orion_residual_block_noalloc(const double* dq, const double* vol,
   if (ntot > (long long)ORION_NOALLOC_MAX_POINTS)
     return na_fail(ORION_E_INVALID, "block has " + std::to_string(ntot) + " interior points; the allocation-free "
                                     "residual accepts at most " + std::to_string(ORION_NOALLOC_MAX_POINTS));
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return na_fail(ORION_E_CUDA, "no current device");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // The call ends with a stream synchronisation, which a capturing stream
+  // cannot take: refuse instead of invalidating the caller's capture.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess)
+    return na_fail(ORION_E_CUDA, "cudaStreamIsCapturing failed on the given stream");
+  if (cap != cudaStreamCaptureStatusNone)
+    return na_fail(ORION_E_INVALID, "orion_residual_block_noalloc waits for its stream and cannot run on a "
+                                    "capturing stream");
+  // The device address of the static array in the current context, looked up
+  // on every call (it allocates nothing, and a cached address would outlive a
+  // device reset or a new primary context).
   NoAllocScratch* scr = nullptr;
   {
-    // one-time set-up per device: the device address of the static array
-    std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_ptr[dev]) {
-      void* p = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess) return na_fail(ORION_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-      g_na_ptr[dev] = static_cast<NoAllocScratch*>(p);
-    }
-    scr = g_na_ptr[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return na_fail(ORION_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    scr = static_cast<NoAllocScratch*>(p);
   }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int npart = (int)((ntot + kNaChunk - 1) / kNaChunk);
   k_noalloc_partials<<<npart, kNaThreads, 0, s>>>(dq, vol, dt, idim, jdim, kdim, scr);
   k_noalloc_final<<<1, 1024, 0, s>>>(scr, npart, idim, jdim);
@@ -144,6 +144,6 @@ extern "C" int orion_residual_block_noalloc(const double* dq, const double* vol,
   out->max = r.max;
   for (int m = 0; m < 5; ++m) out->max_loc[m] = r.loc[m];
   out->pad = 0;
-  out->phydtime = 0.0;
+  out->phydtime = 0.0;  // not computed here: it is the time-step stage's minimum, not a residual statistic
   return 0;
 }

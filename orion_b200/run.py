@@ -1,7 +1,11 @@
-"""Runs a configuration for a few steps, for profilers (ncu launch lists and
-single-kernel captures).
+"""Runs one synthetic configuration through the C ABI and prints its residual
+history: the command-line counterpart of the reference's driver loop
+(src/core/OrionSolver.cpp:139-209) for the bump-channel configurations.
 
-    python -m orion_b200.profile_run --config 1 --steps 2 --warmup 1 --precision mixed
+    python -m orion_b200.run --config 1 --steps 2 --warmup 1 --precision mixed
+    python -m orion_b200.run --config 0 --steps 200 --every 20
+
+Profilers wrap it (a launch list of a few steps, a one-kernel capture).
 """
 from __future__ import annotations
 
@@ -17,6 +21,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "plain"])
     ap.add_argument("--small", action="store_true", help="a 2x2x2-block 97x65x49 case instead")
+    ap.add_argument("--every", type=int, default=0, help="print every n-th step of the history (0: the last)")
     a = ap.parse_args()
     if a.small:
         case = cases.bump_case("profile_small", 97, 65, 49, split=(2, 2, 2), nsteps=a.steps)
@@ -26,6 +31,9 @@ def main():
     fs = solver.FlowFieldSet(case, precision=prec)
     fs.step(a.warmup)
     h = fs.step(a.steps)
+    if a.every > 0:
+        for n in range(a.every - 1, a.steps, a.every):
+            print(f"step {a.warmup + n + 1:6d}  rms {h[n, 0]:.6e}  max {h[n, 1]:.6e}")
     print(f"{case.name} {a.precision}: {a.steps} steps, rms {h[-1, 0]:.6e}")
     fs.close()
 

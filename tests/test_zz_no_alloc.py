@@ -63,3 +63,32 @@ def test_noalloc_residual_rejects_blocks_beyond_its_scratch():
     rc, _ = _noalloc(t, t, t, (205, 205, 205))  # 8,615,125 > ORION_NOALLOC_MAX_POINTS
     assert rc == -1
     assert b"at most" in _lib.load().orion_last_error()
+
+
+def test_noalloc_residual_refuses_a_capturing_stream():
+    import torch
+
+    case = cases.small_case("noalloc_cap", dims=(17, 13, 13), split=(1, 1, 1), noise_seed=3)
+    fs = solver.FlowFieldSet(case)
+    fs.step(1)
+    dq, vol, dt = _device_copies(fs)
+    dims = case.blocks[0].dims
+    rc, _ = _noalloc(dq, vol, dt, dims)  # first call on the device: outside any capture
+    assert rc == 0, _lib.load().orion_last_error()
+    torch.cuda.synchronize()
+    side = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(side):
+        g.capture_begin()
+        try:
+            rc, _ = _noalloc(dq, vol, dt, dims)
+        finally:
+            g.capture_end()
+    assert rc == -1
+    assert b"capturing" in _lib.load().orion_last_error()
+    # the shared scratch still serves the next ordinary call
+    ref = solver.ResidualMonitor.compute(fs)
+    rc, out = _noalloc(dq, vol, dt, dims)
+    assert rc == 0 and abs(out.rms - ref.rms_residual) <= 1e-12 * ref.rms_residual
+    del g
+    fs.close()
