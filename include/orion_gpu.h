@@ -44,6 +44,8 @@ extern "C" {
 #define ORION_SWEEP_PLANES 0   /* one launch per hyperplane */
 #define ORION_SWEEP_GRID 1     /* one cooperative launch, bounded grid barrier per hyperplane */
 #define ORION_SWEEP_CLUSTER 2  /* thread-block clusters (8 or 16 CTAs), cluster barrier per hyperplane */
+#define ORION_SWEEP_TILES 3    /* one launch per pass: 32x4-line tiles, each waiting only on its upstream
+                                  neighbour tiles' progress (bounded waits); the default */
 
 /* BC types (src/bc/PhysicalBC.cpp:576-613) */
 #define ORION_BC_INTERFACE (-1)
@@ -145,8 +147,8 @@ int orion_case_stream(orion_case_t c, void** stream);
 /* Kernel launches one captured step issues (after the first orion_step). */
 int orion_case_step_launches(orion_case_t c, int* n);
 /* How the implicit sweeps are scheduled: out[0] = mode (0 one launch per
- * hyperplane, 1 persistent cooperative grid, 2 thread-block clusters),
- * out[1] = CTAs (grid) or clusters, out[2] = CTAs per cluster, out[3] = threads
+ * hyperplane, 1 persistent cooperative grid, 2 thread-block clusters, 3 tile
+ * wavefront), out[1] = CTAs (grid), clusters or forward tiles, out[2] = CTAs per cluster, out[3] = threads
  * per CTA, out[4] = hyperplanes of the longest sweep.  Waits for set-up only. */
 int orion_case_sweep_schedule(orion_case_t c, int out[5]);
 /* Device bytes held by the case (the HBM footprint used for admission). */

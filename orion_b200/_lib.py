@@ -12,8 +12,8 @@ LIB_PATH = os.environ.get("ORION_GPU_LIB") or os.path.join(HERE, "liborion_gpu.s
 
 PREC_FP64 = 0
 PREC_MIXED = 1
-SWEEP_PLANES, SWEEP_GRID, SWEEP_CLUSTER = 0, 1, 2
-SWEEP_NAMES = {SWEEP_PLANES: "planes", SWEEP_GRID: "grid", SWEEP_CLUSTER: "cluster"}
+SWEEP_PLANES, SWEEP_GRID, SWEEP_CLUSTER, SWEEP_TILES = 0, 1, 2, 3
+SWEEP_NAMES = {SWEEP_PLANES: "planes", SWEEP_GRID: "grid", SWEEP_CLUSTER: "cluster", SWEEP_TILES: "tiles"}
 
 FIELD_PRIM, FIELD_Q, FIELD_DQ, FIELD_METRICS, FIELD_VOL, FIELD_DT, FIELD_C, FIELD_MU = range(8)
 FIELD_NCOMP = {FIELD_PRIM: 6, FIELD_Q: 5, FIELD_DQ: 5, FIELD_METRICS: 9, FIELD_VOL: 1, FIELD_DT: 1,

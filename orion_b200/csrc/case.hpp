@@ -42,6 +42,11 @@ constexpr int kHistCap = 4096;      // residual history ring
 #endif
 constexpr int kSweepThreads = ORION_SWEEP_THREADS;
 constexpr size_t kLineSmemBudget = 96 * 1024;
+// k rows per sweep tile (the tile is 32 j x kTileK k grid lines, one thread each)
+#ifndef ORION_TILE_K
+#define ORION_TILE_K 4
+#endif
+constexpr int kTileK = ORION_TILE_K;
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -69,6 +74,14 @@ struct DeviceLists {
   int* cl_base = nullptr;                        // start of each group's offsets
   int* cl_nplanes = nullptr;                     // hyperplanes of each group
   long long spin_limit = 1LL << 21;              // polls before a grid barrier gives up (about a second)
+  // tile wavefront sweeps (sweep_tiles.cuh): per direction the tile list in
+  // ticket order, and one control block (ticket + progress per tile) reset
+  // before every pass
+  bool tiles_on = false;
+  void* sweep_tiles[2] = {nullptr, nullptr};     // SweepTile lists, forward / backward
+  int n_sweep_tiles[2] = {0, 0};
+  void* tile_ctl = nullptr;                      // TileCtl with max(n_sweep_tiles) progress words
+  size_t tile_ctl_bytes = 0;
   int max_planes = 0;
   long long* halo_src = nullptr;
   long long* halo_dst = nullptr;

@@ -52,8 +52,11 @@ struct BlockDev {
   // Coefficients of the flux splitting that do not involve the swept increment
   // (computed once per step, off the sweeps' critical path):
   S* sk_nrm;              // 9 (static): unit normal nx_n,ny_n,nz_n of the point's xi, eta, zeta metrics
-  S* sk_nbq;              // 6: u, v, w, H, c^2, (gamma-1)/2 v^2 of the point as somebody's neighbour
+  S* sk_nbq;              // 8: u, v, w, H, c^2, (gamma-1)/2 v^2, c, 2 mu/(|Re| rho vol + 1e-30) of the point as
+                          // somebody's neighbour
   S* sk_pair;             // 30: per face neighbour q (lower i,j,k, upper i,j,k): l1, x1, x2, ct_n, rv/2
+  S* sk_gm;               // 3 (static): |grad xi|, |grad eta|, |grad zeta| of the point's metrics
+  S* sk_inv;              // 3 (static): 1 / max(|grad .|, 1e-30)
 };
 
 // Scalar parameters (orion_params_t after conversion).

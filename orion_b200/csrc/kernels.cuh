@@ -1105,6 +1105,9 @@ __global__ void k_skew_static(const BlockDev<S>* __restrict__ blocks, int b) {
       B.sk_nrm[(3 * d) * B.ncomp + c] = nx * inv_mag;
       B.sk_nrm[(3 * d + 1) * B.ncomp + c] = ny * inv_mag;
       B.sk_nrm[(3 * d + 2) * B.ncomp + c] = nz * inv_mag;
+      // the unclamped magnitude the spectral radius uses, and the reciprocal of the clamped one
+      B.sk_gm[d * B.ncomp + c] = sqrt_s(nx * nx + ny * ny + nz * nz);
+      B.sk_inv[d * B.ncomp + c] = inv_mag;
     }
   }
 }
@@ -1113,7 +1116,7 @@ __global__ void k_skew_static(const BlockDev<S>* __restrict__ blocks, int b) {
 // windows zeroed (set_boundary_dq_zero + the AoS copy, StateUpdater.cpp:447-570);
 // diagonal coefficient 1/(1/dt + sum of radii) (get_diag_coeff :267-295), the
 // same in all four sweeps.
-template <typename S, typename T>
+template <typename S, typename T, bool PAIRS = true>
 __global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
@@ -1127,11 +1130,13 @@ __global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk
     const S* pr = FluxSrc<S>::prim(B);
     const T rho = (T)pr[nat], u = (T)pr[np + nat], v = (T)pr[2 * np + nat], w = (T)pr[3 * np + nat],
             p = (T)pr[4 * np + nat];
-    B.sk_prim[c] = (S)rho;
-    B.sk_prim[nc + c] = (S)u;
-    B.sk_prim[2 * nc + c] = (S)v;
-    B.sk_prim[3 * nc + c] = (S)w;
-    B.sk_prim[4 * nc + c] = (S)p;
+    if (PAIRS) {  // the operands of k_sweep_pairs
+      B.sk_prim[c] = (S)rho;
+      B.sk_prim[nc + c] = (S)u;
+      B.sk_prim[2 * nc + c] = (S)v;
+      B.sk_prim[3 * nc + c] = (S)w;
+      B.sk_prim[4 * nc + c] = (S)p;
+    }
     T km[9];
     for (int m = 0; m < 9; ++m) km[m] = (T)B.sk_metrics[m * nc + c];
     const T ra = spectral_radius<T>(rho, u, v, w, p, gamma, km[0], km[1], km[2]);
@@ -1139,10 +1144,17 @@ __global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk
     const T rc = spectral_radius<T>(rho, u, v, w, p, gamma, km[6], km[7], km[8]);
     T rva = T(0), rvb = T(0), rvc = T(0);
     const T mu = (T)B.mu[nat];
-    B.sk_mu[c] = (S)mu;
+    if (PAIRS) B.sk_mu[c] = (S)mu;
+    T vcoef = T(0);
     if (P.nvis == 1) {
       T vol = (T)B.sk_vol[c];
       if (vol < T(1e-30)) vol = T(1e-30);
+      {  // the neighbour factor of visc_spectral_radius (StateUpdater.cpp:194-207)
+        T rc = rho;
+        if (rc < T(1e-30)) rc = T(1e-30);
+        const T rm_vol = rc * vol;
+        vcoef = T(2) * mu / (tabs(reynolds) * rm_vol + T(1.0e-30));
+      }
       rva = visc_spectral_radius<T>(rho, mu, vol, reynolds, km[0], km[1], km[2]);
       rvb = visc_spectral_radius<T>(rho, mu, vol, reynolds, km[3], km[4], km[5]);
       rvc = visc_spectral_radius<T>(rho, mu, vol, reynolds, km[6], km[7], km[8]);
@@ -1165,6 +1177,8 @@ __global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk
       B.sk_nbq[3 * nc + c] = (S)H;
       B.sk_nbq[4 * nc + c] = (S)c2;
       B.sk_nbq[5 * nc + c] = (S)af;
+      B.sk_nbq[6 * nc + c] = (S)tsqrt(c2);
+      B.sk_nbq[7 * nc + c] = (S)vcoef;
     }
   }
 }

@@ -146,20 +146,25 @@ __device__ __forceinline__ T wcns_right(T q_m1, T q_0, T q_p1, T q_p2, T q_p3) {
 // 6th-order / boundary flux differences (FLUX_DXYZ,
 // src/solver/InviscidFluxComputer.cpp:197-233 and src/solver/FluxComputer.cpp:257-296,
 // identical formulas).  f points at face values with stride `st`; point t in [0,ni).
-template <typename T>
-__device__ __forceinline__ T flux_diff(const T* f, int st, int t, int ni) {
+// F(k) is face k's flux (faces 0..ni).
+template <typename T, typename F>
+__device__ __forceinline__ T flux_diff_at(F f, int t, int ni) {
   if (t >= 2 && t < ni - 2) {
-    const T term1 = T(2250) * (f[(t + 1) * st] - f[t * st]);
-    const T term2 = T(-125) * (f[(t + 2) * st] - f[(t - 1) * st]);
-    const T term3 = T(9) * (f[(t + 3) * st] - f[(t - 2) * st]);
+    const T term1 = T(2250) * (f(t + 1) - f(t));
+    const T term2 = T(-125) * (f(t + 2) - f(t - 1));
+    const T term3 = T(9) * (f(t + 3) - f(t - 2));
     return (term1 + term2 + term3) / T(1920);
   }
-  if (t == 0) return (T(-23) * f[0] + T(21) * f[st] + T(3) * f[2 * st] - f[3 * st]) / T(24);
-  if (t == 1) return (f[0] - T(27) * f[st] + T(27) * f[2 * st] - f[3 * st]) / T(24);
-  if (t == ni - 1)
-    return -(T(-23) * f[ni * st] + T(21) * f[(ni - 1) * st] + T(3) * f[(ni - 2) * st] - f[(ni - 3) * st]) / T(24);
+  if (t == 0) return (T(-23) * f(0) + T(21) * f(1) + T(3) * f(2) - f(3)) / T(24);
+  if (t == 1) return (f(0) - T(27) * f(1) + T(27) * f(2) - f(3)) / T(24);
+  if (t == ni - 1) return -(T(-23) * f(ni) + T(21) * f(ni - 1) + T(3) * f(ni - 2) - f(ni - 3)) / T(24);
   // t == ni - 2
-  return -(f[ni * st] - T(27) * f[(ni - 1) * st] + T(27) * f[(ni - 2) * st] - f[(ni - 3) * st]) / T(24);
+  return -(f(ni) - T(27) * f(ni - 1) + T(27) * f(ni - 2) - f(ni - 3)) / T(24);
+}
+
+template <typename T>
+__device__ __forceinline__ T flux_diff(const T* f, int st, int t, int ni) {
+  return flux_diff_at<T>([&](int k) -> T { return f[k * st]; }, t, ni);
 }
 
 // ---------------------------------------------------------------------------

@@ -15,6 +15,7 @@
 #include "metrics_dev.cuh"
 #include "output_dev.cuh"
 #include "shard_dev.cuh"
+#include "sweep_tiles.cuh"
 
 using namespace orion;
 
@@ -75,7 +76,8 @@ size_t block_bytes(const HostBlock& b, size_t ssz) {
   add((npl * b.kdim + 1) * 4);  // koff
   add(nc * 4);                  // sk_nat
   add(6 * nc * 4);              // sk_nb
-  add(72 * nc * ssz);           // sk_metrics 9, sk_vol, sk_prim 5, sk_mu, sk_coed, sk_rhs 5, sk_dq 5, sk_nrm 9, sk_nbq 6, sk_pair 30
+  add(80 * nc * ssz);           // sk_metrics 9, sk_vol, sk_prim 5, sk_mu, sk_coed, sk_rhs 5, sk_dq 5, sk_nrm 9, sk_nbq 8,
+                                // sk_pair 30, sk_gm 3, sk_inv 3
   return align_up(s, 256);
 }
 
@@ -112,7 +114,7 @@ void carve_block(char* base, const HostBlock& b, BlockDev<S>& d) {
   d.koff = reinterpret_cast<int*>(take(((size_t)npl * b.kdim + 1) * 4));
   d.sk_nat = reinterpret_cast<int*>(take(nc * 4));
   d.sk_nb = reinterpret_cast<int*>(take(6 * nc * 4));
-  S* sk = reinterpret_cast<S*>(take(72 * nc * sizeof(S)));
+  S* sk = reinterpret_cast<S*>(take(80 * nc * sizeof(S)));
   d.sk_metrics = sk;
   d.sk_vol = sk + 9 * nc;
   d.sk_prim = sk + 10 * nc;
@@ -122,7 +124,9 @@ void carve_block(char* base, const HostBlock& b, BlockDev<S>& d) {
   d.sk_dq = sk + 22 * nc;
   d.sk_nrm = sk + 27 * nc;
   d.sk_nbq = sk + 36 * nc;
-  d.sk_pair = sk + 42 * nc;
+  d.sk_pair = sk + 44 * nc;
+  d.sk_gm = sk + 74 * nc;
+  d.sk_inv = sk + 77 * nc;
   d.ni = b.idim;
   d.nj = b.jdim;
   d.nk = b.kdim;
@@ -283,6 +287,73 @@ int build_line_tiles(orion_case_t c) {
     if ((rc = dev_upload(c, &L.tiles[d], tiles))) return rc;
     L.n_tiles[d] = (int)tiles.size();
   }
+  return 0;
+}
+
+// Tile wavefront sweeps: tiles of 32 x kTileK grid lines, per direction in
+// ticket order.  A tile's start in steps is 32 J + kTileK K behind its
+// block's first tile, and its upstream tiles (J-1, K) and (J, K-1) start
+// strictly earlier, so ordering by start offset (ties by block, then J) is a
+// dependency-respecting order for every block at once.
+int build_sweep_tiles(orion_case_t c) {
+  auto& L = c->L;
+  constexpr int TJ = 32, TK = kTileK;
+  int maxn = 0;
+  for (int dir = 0; dir < 2; ++dir) {
+    struct Item {
+      int start, block, J, K;
+    };
+    std::vector<Item> items;
+    std::vector<int> first(c->nblocks + 1, 0);
+    for (int b = 0; b < c->nblocks; ++b) {
+      const auto& h = c->hb[b];
+      const int nJ = (h.jdim + TJ - 1) / TJ, nK = (h.kdim + TK - 1) / TK;
+      for (int K = 0; K < nK; ++K)
+        for (int J = 0; J < nJ; ++J) items.push_back(Item{TJ * J + TK * K, b, J, K});
+    }
+    std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) {
+      if (a.start != b.start) return a.start < b.start;
+      if (a.block != b.block) return a.block < b.block;
+      return a.J < b.J;
+    });
+    // slot of (block, J, K)
+    std::vector<long long> base(c->nblocks + 1, 0);
+    std::vector<int> nJs(c->nblocks);
+    for (int b = 0; b < c->nblocks; ++b) {
+      const auto& h = c->hb[b];
+      nJs[b] = (h.jdim + TJ - 1) / TJ;
+      base[b + 1] = base[b] + (long long)nJs[b] * ((h.kdim + TK - 1) / TK);
+    }
+    std::vector<int> slot_of((size_t)base[c->nblocks], -1);
+    for (size_t q = 0; q < items.size(); ++q)
+      slot_of[(size_t)(base[items[q].block] + (long long)items[q].K * nJs[items[q].block] + items[q].J)] = (int)q;
+    std::vector<SweepTile> tiles(items.size());
+    for (size_t q = 0; q < items.size(); ++q) {
+      const Item& it = items[q];
+      const auto& h = c->hb[it.block];
+      SweepTile& w = tiles[q];
+      w = SweepTile{};
+      w.block = it.block;
+      w.jb = dir == 0 ? it.J * TJ : h.jdim - 1 - it.J * TJ;
+      w.kb = dir == 0 ? it.K * TK : h.kdim - 1 - it.K * TK;
+      const long long bb = base[it.block];
+      w.up_j = it.J > 0 ? slot_of[(size_t)(bb + (long long)it.K * nJs[it.block] + it.J - 1)] : -1;
+      w.up_k = it.K > 0 ? slot_of[(size_t)(bb + (long long)(it.K - 1) * nJs[it.block] + it.J)] : -1;
+      if ((w.up_j >= 0 && w.up_j >= (int)q) || (w.up_k >= 0 && w.up_k >= (int)q))
+        return fail(ORION_E_INVALID, "sweep tile order does not respect the dependencies");
+    }
+    int rc;
+    SweepTile* d = nullptr;
+    if ((rc = dev_upload(c, &d, tiles))) return rc;
+    L.sweep_tiles[dir] = d;
+    L.n_sweep_tiles[dir] = (int)tiles.size();
+    maxn = std::max(maxn, (int)tiles.size());
+  }
+  L.tile_ctl_bytes = offsetof(TileCtl, progress) + sizeof(unsigned int) * (size_t)maxn;
+  unsigned char* ctl = nullptr;
+  int rc;
+  if ((rc = dev_alloc(c, &ctl, L.tile_ctl_bytes))) return rc;
+  L.tile_ctl = ctl;
   return 0;
 }
 
@@ -464,6 +535,7 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off, const Ex
     if ((rc = dev_alloc(c, &ctl, 4))) return rc;
     L.sweep_ctl = ctl;
   }
+  if ((rc = build_sweep_tiles(c))) return rc;
   return 0;
 }
 
@@ -830,7 +902,9 @@ int orion_case_set_params(orion_case_t c, const orion_params_t* params) {
 }
 
 static void current_schedule(orion_case_t c, orion_schedule_t* s) {
-  s->sweep_form = c->L.cl_size > 0 ? ORION_SWEEP_CLUSTER : (c->L.persist_grid > 0 ? ORION_SWEEP_GRID : ORION_SWEEP_PLANES);
+  s->sweep_form = c->L.tiles_on ? ORION_SWEEP_TILES
+                  : c->L.cl_size > 0 ? ORION_SWEEP_CLUSTER
+                  : (c->L.persist_grid > 0 ? ORION_SWEEP_GRID : ORION_SWEEP_PLANES);
   s->cluster_size = c->L.cl_size;
   s->lanes = c->L.lanes_cap;
   s->ms_per_step = 0.f;
@@ -944,8 +1018,9 @@ int orion_case_autotune(orion_case_t c, int steps_per_trial, orion_schedule_t* t
     rc = trial(s);
   }
   // phase 2: every sweep form, with the best lanes
-  const orion_schedule_t forms[4] = {{ORION_SWEEP_CLUSTER, 16, 0, 0.f}, {ORION_SWEEP_CLUSTER, 8, 0, 0.f},
-                                     {ORION_SWEEP_GRID, 0, 0, 0.f}, {ORION_SWEEP_PLANES, 0, 0, 0.f}};
+  const orion_schedule_t forms[5] = {{ORION_SWEEP_TILES, 0, 0, 0.f}, {ORION_SWEEP_CLUSTER, 16, 0, 0.f},
+                                     {ORION_SWEEP_CLUSTER, 8, 0, 0.f}, {ORION_SWEEP_GRID, 0, 0, 0.f},
+                                     {ORION_SWEEP_PLANES, 0, 0, 0.f}};
   for (const auto& f : forms) {
     if (rc) break;
     if (f.sweep_form == start.sweep_form && (f.sweep_form != ORION_SWEEP_CLUSTER || f.cluster_size == start.cluster_size))
@@ -998,10 +1073,10 @@ int orion_case_step_launches(orion_case_t c, int* n) {
 int orion_case_sweep_schedule(orion_case_t c, int out[5]) {
   if (!c || !out) return fail(ORION_E_INVALID, "null argument");
   const auto& L = c->L;
-  out[0] = L.cl_size > 0 ? 2 : (L.persist_grid > 0 ? 1 : 0);
-  out[1] = L.cl_size > 0 ? L.cl_count : L.persist_grid;
+  out[0] = L.tiles_on ? 3 : (L.cl_size > 0 ? 2 : (L.persist_grid > 0 ? 1 : 0));
+  out[1] = L.tiles_on ? L.n_sweep_tiles[0] : (L.cl_size > 0 ? L.cl_count : L.persist_grid);
   out[2] = L.cl_size;
-  out[3] = L.sweep_nt;
+  out[3] = L.tiles_on ? 32 * kTileK : L.sweep_nt;
   out[4] = L.max_planes;
   return 0;
 }
@@ -1226,7 +1301,7 @@ static int sweep_status(orion_case_t c) {
   if (ctl[1]) {
     CUDA_TRY(cudaMemsetAsync(c->L.sweep_ctl, 0, sizeof(ctl), c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
-    return fail(ORION_E_TIMEOUT, "a grid barrier of the implicit sweeps gave up waiting");
+    return fail(ORION_E_TIMEOUT, "a bounded wait of the implicit sweeps (grid barrier or tile progress) gave up waiting");
   }
   return 0;
 }

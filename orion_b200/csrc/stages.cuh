@@ -6,6 +6,7 @@
 
 #include "case.hpp"
 #include "kernels.cuh"
+#include "sweep_tiles.cuh"
 
 namespace orion {
 
@@ -27,6 +28,12 @@ struct Stages {
 
   static int set_line_attributes() {
     const int b = (int)kLineSmemBudget;
+    CUDA_TRY(cudaFuncSetAttribute(k_sweep_tiles<S, T, SW_LUSGS_FWD, 1, kTileK>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CUDA_TRY(cudaFuncSetAttribute(k_sweep_tiles<S, T, SW_LUSGS_BWD, -1, kTileK>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CUDA_TRY(cudaFuncSetAttribute(k_sweep_tiles<S, T, SW_GS, 1, kTileK>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CUDA_TRY(cudaFuncSetAttribute(k_sweep_tiles<S, T, SW_GS, -1, kTileK>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
     CUDA_TRY(cudaFuncSetAttribute(k_viscous<0, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
     CUDA_TRY(cudaFuncSetAttribute(k_viscous<1, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
     CUDA_TRY(cudaFuncSetAttribute(k_viscous<2, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
@@ -232,11 +239,12 @@ struct Stages {
     return 0;
   }
 
-  // An explicit sweep form (ORION_SWEEP_PLANES / _GRID / _CLUSTER with size cs).
+  // An explicit sweep form (ORION_SWEEP_TILES / _PLANES / _GRID / _CLUSTER with size cs).
   static int schedule(orion_case_t c, int form, int cs) {
     c->L.persist_grid = 0;
     c->L.cl_size = 0;
-    if (form == ORION_SWEEP_PLANES) return 0;
+    c->L.tiles_on = form == ORION_SWEEP_TILES;
+    if (form == ORION_SWEEP_PLANES || form == ORION_SWEEP_TILES) return 0;
     if (form == ORION_SWEEP_GRID) {
       int rc = grid_setup(c);
       if (rc) return rc;
@@ -254,12 +262,17 @@ struct Stages {
   static int persistent_grid(orion_case_t c) {
     c->L.persist_grid = 0;
     c->L.cl_size = 0;
+    c->L.tiles_on = false;
     // default: one programmatic-dependent launch per hyperplane (the fastest
     // form the autotuner measured on the configurations, both precisions)
     const char* env = getenv("ORION_SWEEP");
     const std::string mode = env ? std::string(env) : std::string("planes");
-    const char* lim = getenv("ORION_SWEEP_SPIN_LIMIT");  // bound of the grid barrier's wait
+    const char* lim = getenv("ORION_SWEEP_SPIN_LIMIT");  // bound of the sweeps' device waits
     if (lim) c->L.spin_limit = atoll(lim);
+    if (mode == "tiles") {
+      c->L.tiles_on = true;
+      return 0;
+    }
     if (mode == "planes") return 0;
     if (mode == "cluster") {
       int rc = cluster_setup<kSweepThreads>(c);
@@ -312,11 +325,38 @@ struct Stages {
     return 0;
   }
 
+  // One pass of the tile wavefront: reset the tickets and progress words, then
+  // one CTA per tile.
+  template <int MODE, int DIR>
+  static int tile_pass(orion_case_t c) {
+    auto& L = c->L;
+    const int d = DIR > 0 ? 0 : 1;
+    const int n = L.n_sweep_tiles[d];
+    if (n <= 0) return 0;
+    CUDA_TRY(cudaMemsetAsync(L.tile_ctl, 0, offsetof(TileCtl, progress) + sizeof(unsigned int) * (size_t)n,
+                             c->stream));
+    SweepCtl* sc = static_cast<SweepCtl*>(L.sweep_ctl);
+    k_sweep_tiles<S, T, MODE, DIR, kTileK><<<n, 32 * kTileK + 32, tile_ring_bytes<T, MODE, kTileK>(), c->stream>>>(
+        blocks(c), static_cast<const SweepTile*>(L.sweep_tiles[d]), n, static_cast<TileCtl*>(L.tile_ctl),
+        &sc->error, c->P, L.spin_limit);
+    return 0;
+  }
+
   static int update(orion_case_t c, bool fuse_residual) {
     auto& L = c->L;
-    k_lusgs_prep<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
-    k_sweep_pairs<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
-    if (L.cl_size > 0) {
+    if (L.tiles_on) {
+      k_lusgs_prep<S, T, false><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
+    } else {
+      k_lusgs_prep<S, T, true><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
+      k_sweep_pairs<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
+    }
+    if (L.tiles_on) {
+      int rc = tile_pass<SW_LUSGS_FWD, 1>(c);
+      if (!rc) rc = tile_pass<SW_LUSGS_BWD, -1>(c);
+      if (!rc) rc = tile_pass<SW_GS, 1>(c);
+      if (!rc) rc = tile_pass<SW_GS, -1>(c);
+      if (rc) return rc;
+    } else if (L.cl_size > 0) {
       int rc = sweeps_cluster_nt<kSweepThreads>(c);
       if (rc) return rc;
     } else if (L.persist_grid > 0) {

@@ -149,7 +149,7 @@ class FlowFieldSet:
     def sweep_schedule(self) -> dict:
         v = (C.c_int * 5)()
         check(_lib.load().orion_case_sweep_schedule(self._h, v))
-        mode = {0: "planes", 1: "grid", 2: "cluster"}[v[0]]
+        mode = _lib.SWEEP_NAMES[v[0]]
         return {"mode": mode, "units": v[1], "cluster_size": v[2], "threads": v[3], "hyperplanes": v[4]}
 
     def footprint(self) -> int:
@@ -207,7 +207,7 @@ class FlowFieldSet:
         return {"sweep": _lib.SWEEP_NAMES[s.sweep_form], "cluster_size": s.cluster_size, "lanes": s.lanes}
 
     def set_schedule(self, sweep: str, cluster_size: int = 0, lanes: int = 32):
-        """Fixes the step schedule: sweep form (planes | grid | cluster), cluster size
+        """Fixes the step schedule: sweep form (tiles | planes | grid | cluster), cluster size
         (8, 16, 0 = largest co-resident) and grid lines per CTA of the line kernels."""
         form = {v: k for k, v in _lib.SWEEP_NAMES.items()}[sweep]
         s = _lib.Schedule(form, cluster_size, lanes, 0.0)

@@ -4,6 +4,10 @@ small seeded cases.
 
     make -C oracle ref && python tests/golden/gen_golden.py [fixture ...]
 
+With no arguments it regenerates the small fixtures; the configuration
+horizons (c0_200, c1_40: minutes of reference CPU time) are made only when
+named.
+
 Each fixture holds the case recipe, the reference's residual history
 (rms, max, max location, phydtime per step) and its final primitive state:
 the full interior state for a single-block case, every 7th interior point
@@ -57,7 +61,48 @@ def interior_prim(state, sub: int = 1) -> np.ndarray:
     return flat[:, ::sub]
 
 
+# The benchmark configurations at their own horizons (cases.config):
+#   c0_200: config 0 (one block 97x49x33) for its 200 steps;
+#   c1_40:  config 1 (eight blocks 193x97x65, split 2x2x2) for 40 steps, and the
+#           reference's residual history over its 300 steps (hist_long), which
+#           records where the reference's own scheme leaves convergence on this
+#           split.
+# The state is stored sub-sampled, with per-variable sums and sums of squares
+# of the whole interior state beside it.
+HORIZONS = {
+    "c0_200": dict(config=0, nsteps=200, sub=37, long_steps=0),
+    "c1_40": dict(config=1, nsteps=40, sub=211, long_steps=300),
+}
+
+
+def state_sums(flat: np.ndarray) -> np.ndarray:
+    """Per-variable sum and sum of squares of the interior state (5 x 2)."""
+    return np.stack([flat.sum(axis=1), (flat * flat).sum(axis=1)], axis=1)
+
+
+def horizon(key: str, spec: dict) -> None:
+    case = cases.config(spec["config"], nsteps=spec["nsteps"])
+    tmp = tempfile.mkdtemp(prefix="golden_")
+    cdir = os.path.join(tmp, "case")
+    case.write_reference_inputs(cdir)
+    refio.run_reference(cdir, case.nsteps, os.path.join(tmp, "out"))
+    hist = refio.read_hist(os.path.join(tmp, "out", "hist.bin"))
+    final = refio.read_state(os.path.join(tmp, "out", "final.bin"))
+    flat = interior_prim(final, 1)
+    extra = {}
+    if spec["long_steps"]:
+        refio.run_reference(cdir, spec["long_steps"], os.path.join(tmp, "long"), time_only=True)
+        extra["hist_long"] = refio.read_hist(os.path.join(tmp, "long", "hist.bin"))
+    np.savez_compressed(os.path.join(HERE, key + ".npz"), hist=hist, prim=flat[:, ::spec["sub"]],
+                        sums=state_sums(flat), sub=np.array([spec["sub"]]),
+                        recipe=np.array([json.dumps(spec)]), **extra)
+    print(key, case.npoints, "points", case.nsteps, "steps", hist[-1, :2])
+
+
 def main(keys=None):
+    for key, spec in HORIZONS.items():
+        if keys and key in keys:
+            horizon(key, spec)
     for key, recipe in RECIPES.items():
         if keys and key not in keys:
             continue

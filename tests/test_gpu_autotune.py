@@ -1,7 +1,8 @@
 """Step schedules and the autotuner.
 
-Every schedule (sweep form: per-hyperplane launches, cooperative grid,
-clusters of 8 or 16 CTAs; 8/16/32 grid lines per CTA in the line kernels)
+Every schedule (sweep form: tile wavefront, per-hyperplane launches,
+cooperative grid, clusters of 8 or 16 CTAs; 8/16/32 grid lines per CTA in the
+line kernels)
 keeps the reference's Gauss-Seidel order and the per-point arithmetic, so on
 the plain FP64 path the results are bit-identical whatever the schedule; on
 the mixed path they agree within the mixed tolerance (1e-6 relative L2).
@@ -14,7 +15,7 @@ from orion_b200 import _lib, cases, solver
 
 pytestmark = pytest.mark.gpu
 
-SCHEDULES = [("planes", 0, 32), ("grid", 0, 8), ("cluster", 16, 16), ("cluster", 8, 32)]
+SCHEDULES = [("planes", 0, 32), ("tiles", 0, 16), ("grid", 0, 8), ("cluster", 16, 16), ("cluster", 8, 32)]
 
 
 def _case():

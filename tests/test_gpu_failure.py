@@ -36,3 +36,28 @@ def test_grid_barrier_timeout_is_reported_and_the_context_survives():
     assert np.array_equal(a.step(3), b.step(3))
     a.close()
     b.close()
+
+
+def test_tile_wavefront_wait_timeout_is_reported_and_the_context_survives():
+    """The tile wavefront's waits on its upstream tiles are bounded too: with a
+    limit of one poll a tile that finds its upstream tile behind gives up, the
+    error word stops every other waiting tile, and the host reports
+    ORION_E_TIMEOUT.  The case is made of blocks wide enough in j and k to hold
+    several tiles each, so that tiles do wait on one another."""
+    case = cases.small_case("timeout_tiles", dims=(33, 70, 25), split=(1, 1, 1), noise_seed=5)
+    os.environ["ORION_SWEEP_SPIN_LIMIT"] = "1"
+    try:
+        fs = solver.FlowFieldSet(case, precision=_lib.PREC_FP64)
+    finally:
+        del os.environ["ORION_SWEEP_SPIN_LIMIT"]
+    fs.set_schedule("tiles", 0, 32)
+    with pytest.raises(OrionError) as err:
+        fs.step(1)
+    assert "-6" in str(err.value)
+    fs.close()
+    a = solver.FlowFieldSet(case, precision=_lib.PREC_FP64)
+    b = solver.FlowFieldSet(case, precision=_lib.PREC_FP64)
+    b.set_schedule("planes", 0, 32)
+    assert np.array_equal(a.step(3), b.step(3))
+    a.close()
+    b.close()
