@@ -56,11 +56,14 @@ STEP_BYTES = (1912, 1444)
 # bound); scaled to the bench workload by its point count.
 UPDATE_DRAM_BYTES_PER_POINT_MIXED = 1734.2e6 / 1254792
 
-# The mixed state is compared with the plain FP64 state after this many steps
-# from the same initial state.  On the multi-block configurations the
-# reference's own scheme (and so the plain path, which reproduces it) stops
-# converging after about 15 steps, so the comparison is taken before that.
+# The mixed state is compared with the plain FP64 state from the same initial
+# state at several horizons: on the bench workload (transonic, 64 blocks, whose
+# flow the reference's own scheme does not converge) and on configuration 0
+# (one block, converging).
 L2_STEPS = 10
+L2_HORIZONS = {"workload": (10, 30, 50), "c0_97x49x33": (10, 50, 100, 200)}
+# the reference-CPU leg of the line: timed steps after warm-up steps per process
+CPU_STEPS, CPU_WARMUP = 5, 2
 
 
 def hbm_peak():
@@ -342,7 +345,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ncpu = os.cpu_count() or 1
-        cpu, err = reference_sample(case, 1, 0, min(ncpu, len(case.blocks)))
+        cpu, err = reference_sample(case, CPU_STEPS, CPU_WARMUP, min(ncpu, len(case.blocks)))
         if cpu is None:
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": err}
 

@@ -109,6 +109,7 @@ typedef struct {
 } orion_residual_t;
 
 typedef struct orion_case_s* orion_case_t;
+typedef struct orion_group_s* orion_group_t;
 
 /* A step schedule: sweep form, cluster size (CLUSTER form: 8 or 16; 0 = the
  * largest co-resident) and the grid lines per CTA of the viscous and inviscid
@@ -237,6 +238,29 @@ int orion_case_autotune(orion_case_t c, int steps_per_trial, orion_schedule_t* t
  * the next poll).  It never waits. */
 int orion_step_submit(orion_case_t c, int nsteps);
 int orion_case_poll(orion_case_t c, orion_residual_t* out, int cap, int* n);
+
+/* Groups of cases: many cases, one launch per stage ------------------------
+ * No single counterpart in the reference, which steps the blocks of one case
+ * one after another in every stage (StateUpdater.cpp:544-580,
+ * InviscidFluxComputer.cpp:524-541, FluxComputer.cpp:724-732).  A group steps
+ * several device-resident cases together: every stage is one launch over the
+ * blocks of all members (the sweeps: one launch per hyperplane, or per pass
+ * in the tile form when every member uses it), each block with its own
+ * case's parameters; the residual and time-step reductions run per member,
+ * into the member's own history.  A member's results are bit-identical to
+ * stepping it alone.  The members share one precision and are all viscous or
+ * all Euler; they have no unpolled submitted steps; a case joins at most one
+ * group.  While in a group a case enqueues on the group's stream, so
+ * orion_case_poll and the per-case calls follow the group's launches; destroy
+ * the group before destroying or re-grouping its cases.
+ * orion_group_submit enqueues nsteps group steps (one CUDA graph per step)
+ * and each member's history copy, and returns at once; poll each member with
+ * orion_case_poll.  orion_group_sync waits for the group's stream. */
+int orion_group_create(int n, const orion_case_t* cases, orion_group_t* out);
+int orion_group_submit(orion_group_t g, int nsteps);
+int orion_group_sync(orion_group_t g);
+int orion_group_step_launches(orion_group_t g, int* n);
+int orion_group_destroy(orion_group_t g);
 
 /* Allocation-free residual norm of one block ------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc

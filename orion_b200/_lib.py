@@ -71,6 +71,11 @@ SIGNATURES = {
                                       C.POINTER(Schedule)]),
     "orion_case_grid_metrics": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "orion_case_poll": (C.c_int, [C.c_void_p, C.POINTER(Residual), C.c_int, C.POINTER(C.c_int)]),
+    "orion_group_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    "orion_group_submit": (C.c_int, [C.c_void_p, C.c_int]),
+    "orion_group_sync": (C.c_int, [C.c_void_p]),
+    "orion_group_step_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "orion_group_destroy": (C.c_int, [C.c_void_p]),
     "orion_case_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "orion_case_sync": (C.c_int, [C.c_void_p]),
     "orion_case_footprint": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),

@@ -42,15 +42,20 @@ constexpr int kHistCap = 4096;      // residual history ring
 #endif
 constexpr int kSweepThreads = ORION_SWEEP_THREADS;
 constexpr size_t kLineSmemBudget = 96 * 1024;
-// k rows per sweep tile (the tile is 32 j x kTileK k grid lines, one thread each)
-#ifndef ORION_TILE_K
-#define ORION_TILE_K 4
-#endif
-constexpr int kTileK = ORION_TILE_K;
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// What a group of cases stepped together needs beyond the lists (orion_group_*).
+struct GroupRun {
+  GroupMember* members = nullptr;  // device array, one per case
+  int nmembers = 0;
+  unsigned long long* halo_src = nullptr;  // halo copy as element addresses (the arenas differ)
+  unsigned long long* halo_dst = nullptr;
+  int n_halo = 0;
+};
+
 struct DeviceLists {
+  const GroupRun* group = nullptr;  // set on a group's lists: the stages reduce per case
   Chunk* pad_chunks = nullptr;
   int n_pad_chunks = 0;
   Chunk* int_chunks = nullptr;
@@ -60,6 +65,7 @@ struct DeviceLists {
   int lanes[3] = {1, 1, 1};
   int lanes_cap = 32;                            // line tiles: at most this many grid lines per CTA (set at creation)
   int lmax[3] = {0, 0, 0};
+  int line_units[3] = {0, 0, 0};                 // line tiles' face slots (lanes x (longest line + 1)) of shared memory
   Chunk* sweep_chunks[2] = {nullptr, nullptr};  // forward / backward hyperplane launches
   std::vector<int> sweep_off[2];                 // host: chunk range of each launch
   int* sweep_off_dev[2] = {nullptr, nullptr};    // device copies of sweep_off
@@ -82,6 +88,7 @@ struct DeviceLists {
   int n_sweep_tiles[2] = {0, 0};
   void* tile_ctl = nullptr;                      // TileCtl with max(n_sweep_tiles) progress words
   size_t tile_ctl_bytes = 0;
+  int tile_k = 4;                                // k rows per tile (32 j rows)
   int max_planes = 0;
   long long* halo_src = nullptr;
   long long* halo_dst = nullptr;
@@ -150,6 +157,17 @@ struct orion_case_s {
   long long hist_count = -1;                // device history counter; -1 = not known on the host
   long long pending_first = 0;
   int pending_n = 0;
+  struct orion_group_s* group = nullptr;  // the group the case steps in, if any
+};
+
+// A group of cases stepped together: one launch per stage over all of their
+// blocks.  `proxy` is a case object whose lists, block descriptors and stream
+// are the group's; the stage launchers run it as they run a case.
+struct orion_group_s {
+  std::vector<orion_case_t> members;
+  std::vector<cudaStream_t> saved_streams;  // the members' own streams, given back on destroy
+  orion_case_s* proxy = nullptr;
+  orion::GroupRun run;
 };
 
 namespace orion {

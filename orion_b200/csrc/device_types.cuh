@@ -6,6 +6,8 @@ namespace orion {
 
 constexpr int NG = 3;  // ghost layers (src/preprocess/FlowField.cpp:9-16)
 
+struct ParamsDev;
+
 // One block's device arrays.  Every field is the reference's padded layout
 // (i fastest, component slowest, component stride npad).  S is the storage
 // type of the fields whose precision the mixed path lowers (dq, rhs, dt, c,
@@ -57,6 +59,9 @@ struct BlockDev {
   S* sk_pair;             // 30: per face neighbour q (lower i,j,k, upper i,j,k): l1, x1, x2, ct_n, rv/2
   S* sk_gm;               // 3 (static): |grad xi|, |grad eta|, |grad zeta| of the point's metrics
   S* sk_inv;              // 3 (static): 1 / max(|grad .|, 1e-30)
+  // the block's case parameters when it is stepped in a group of cases
+  // (orion_group_*); nullptr in a case's own descriptors, whose launches pass them
+  const ParamsDev* params;
 };
 
 // Scalar parameters (orion_params_t after conversion).
@@ -116,6 +121,20 @@ struct ResidualOut {
   int loc[5];
   int pad;
   double phydtime;
+};
+
+// One case of a group stepped together: where its blocks, its chunks'
+// partial results and its result slots are.
+struct GroupMember {
+  const void* blocks;            // the case's block descriptors in the group's array
+  int nblocks;
+  int part_off, part_n;          // its interior chunks (residual partials)
+  int pad_off, pad_n;            // its padded chunks (time-step minima)
+  long long total_points;        // interior points x 5
+  unsigned long long* dtmin;     // the case's phydtime slot
+  ResidualOut* hist;             // the case's history ring
+  int* counter;
+  ResPartial* total;
 };
 
 }  // namespace orion

@@ -28,6 +28,13 @@ template <> struct FluxSrc<float> {
 };
 
 
+// The parameters of a block's case: its own copy when the block belongs to a
+// group of cases stepped together, else the launch's.
+template <typename S>
+__device__ __forceinline__ const ParamsDev& block_params(const BlockDev<S>& B, const ParamsDev& launch) {
+  return B.params ? *B.params : launch;
+}
+
 template <typename S>
 __device__ __forceinline__ long long lin(const BlockDev<S>& B, int i, int j, int k) {
   return (long long)i + (long long)B.nx * ((long long)j + (long long)B.ny * (long long)k);
@@ -69,6 +76,13 @@ static __global__ void k_halo_copy(double* __restrict__ arena, const long long* 
   if (t < n) arena[dst[t]] = arena[src[t]];
 }
 
+// The same copy for a group of cases, whose arenas differ: element addresses.
+static __global__ void k_halo_copy_abs(const unsigned long long* __restrict__ src,
+                                       const unsigned long long* __restrict__ dst, int n) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) *reinterpret_cast<double*>(dst[t]) = *reinterpret_cast<const double*>(src[t]);
+}
+
 // ===========================================================================
 // Physical BCs (src/bc/PhysicalBC.cpp:12-613).  One launch per phase; phase p
 // holds the p-th physical region of every block (regions of one block are
@@ -102,11 +116,12 @@ __device__ __forceinline__ void dif_average(const BlockDev<S>& B, long long idx0
 
 template <typename S>
 __global__ void k_bc_phase(const BlockDev<S>* __restrict__ blocks, const RegionDev* __restrict__ regions,
-                           const int* __restrict__ phase_regions, ParamsDev P) {
+                           const int* __restrict__ phase_regions, ParamsDev P_launch) {
   const RegionDev R = regions[phase_regions[blockIdx.y]];
   const int pt = blockIdx.x * blockDim.x + threadIdx.x;
   if (pt >= R.npts) return;
   const BlockDev<S> B = blocks[R.block];
+  const ParamsDev& P = block_params(B, P_launch);
   const int wi = R.hi[0] - R.lo[0] + 1, wj = R.hi[1] - R.lo[1] + 1;
   const int i = R.lo[0] + pt % wi;
   const int j = R.lo[1] + (pt / wi) % wj;
@@ -416,8 +431,16 @@ __device__ __forceinline__ void block_min_to(double v, double* part) {
 }
 
 // phydtime = min(1000, min over the partials) (TimeIntegrator.cpp:151-176), stored as bits.
+__device__ __forceinline__ void dtmin_final_body(const double* __restrict__ part, int n,
+                                                 unsigned long long* __restrict__ dtmin_bits);
+
 static __global__ void __launch_bounds__(1024) k_dtmin_final(const double* __restrict__ part, int n,
                                                              unsigned long long* __restrict__ dtmin_bits) {
+  dtmin_final_body(part, n, dtmin_bits);
+}
+
+__device__ __forceinline__ void dtmin_final_body(const double* __restrict__ part, int n,
+                                                 unsigned long long* __restrict__ dtmin_bits) {
   double v = 1000.0;
   for (int t = threadIdx.x; t < n; t += 1024) v = fmin(v, part[t]);
   for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, off));
@@ -433,10 +456,11 @@ static __global__ void __launch_bounds__(1024) k_dtmin_final(const double* __res
 }
 
 template <typename S, bool DO_Q, bool DO_DT>
-__global__ void k_state(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P,
+__global__ void k_state(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P_launch,
                         double* __restrict__ dt_part) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
+  const ParamsDev& P = block_params(B, P_launch);
   double local_min = 1000.0;
 #pragma unroll 4
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
@@ -463,10 +487,11 @@ __global__ void k_state(const BlockDev<S>* __restrict__ blocks, const Chunk* __r
 
 // time step alone (per-stage entry point): interior points of interior chunks
 template <typename S>
-__global__ void k_timestep(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P,
+__global__ void k_timestep(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P_launch,
                            double* __restrict__ dt_part) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
+  const ParamsDev& P = block_params(B, P_launch);
   double local_min = 1000.0;
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
     const long long n = ch.start + t;  // interior index
@@ -667,11 +692,12 @@ template <> struct LineMinBlocks<float> { static constexpr int visc = ORION_VISC
 template <> struct LineMinBlocks<double> { static constexpr int visc = ORION_VISC_MINB_F64, inv = ORION_INV_MINB_F64; };
 
 template <int D, typename S, typename T>
-__global__ void __launch_bounds__(256, LineMinBlocks<T>::visc) k_viscous(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles, ParamsDev P) {
+__global__ void __launch_bounds__(256, LineMinBlocks<T>::visc) k_viscous(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles, ParamsDev P_launch) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* fsh = reinterpret_cast<T*>(smem_raw);
   const LineTile tl = tiles[blockIdx.x];
   const BlockDev<S> B = blocks[tl.block];
+  const ParamsDev& P = block_params(B, P_launch);
   const int L = dim_along(B, D);
   const int nf = L + 1;
   const long long st = stride_along(B, D);
@@ -943,11 +969,12 @@ __device__ void cascade_right(const BlockDev<S>& B, const InvLine<S, T>& ln, int
 }
 
 template <int D, typename S, typename T>
-__global__ void __launch_bounds__(256, LineMinBlocks<T>::inv) k_inviscid(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles, ParamsDev P) {
+__global__ void __launch_bounds__(256, LineMinBlocks<T>::inv) k_inviscid(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles, ParamsDev P_launch) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* fsh = reinterpret_cast<T*>(smem_raw);
   const LineTile tl = tiles[blockIdx.x];
   const BlockDev<S> B = blocks[tl.block];
+  const ParamsDev& P = block_params(B, P_launch);
   const int L = dim_along(B, D);
   const int nf = L + 1;
   const long long st = stride_along(B, D);
@@ -1117,9 +1144,10 @@ __global__ void k_skew_static(const BlockDev<S>* __restrict__ blocks, int b) {
 // diagonal coefficient 1/(1/dt + sum of radii) (get_diag_coeff :267-295), the
 // same in all four sweeps.
 template <typename S, typename T, bool PAIRS = true>
-__global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P) {
+__global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P_launch) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
+  const ParamsDev& P = block_params(B, P_launch);
   const long long np = B.npad, nc = B.ncomp;
   const T gamma = T(P.gamma), reynolds = T(P.reynolds);
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
@@ -1189,9 +1217,10 @@ __global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk
 // x1, x2), ct_n, and half the viscous radius.  q = 0..2 lower i,j,k (sign +1),
 // q = 3..5 upper (sign -1).
 template <typename S, typename T>
-__global__ void k_sweep_pairs(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P) {
+__global__ void k_sweep_pairs(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P_launch) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
+  const ParamsDev& P = block_params(B, P_launch);
   const long long nc = B.ncomp;
   const T gamma = T(P.gamma);
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
@@ -1402,13 +1431,14 @@ __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefe
 #endif
 template <typename S, typename T, int MODE, int NT>
 __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
-                                                    const Chunk* __restrict__ chunks, ParamsDev P) {
+                                                    const Chunk* __restrict__ chunks, ParamsDev P_launch) {
   constexpr int Q0 = MODE == SW_LUSGS_BWD ? 3 : 0;
   constexpr int Q1 = MODE == SW_LUSGS_FWD ? 3 : 6;
   constexpr bool PRELOAD = sizeof(T) == 4;  // FP32: every static operand in registers before the wait
   const Chunk ch = chunks[blockIdx.x];
   const bool active = (int)threadIdx.x < ch.count;
   const BlockDev<S>& B = blocks[ch.block];
+  const ParamsDev& P = block_params(B, P_launch);
   const long long nc = B.ncomp;
   const int c = (int)ch.start + threadIdx.x;
   // pointers into registers now: griddepcontrol.wait clobbers memory, so
@@ -1727,13 +1757,14 @@ __device__ __forceinline__ void block_reduce_res(double& sum, double& mx, long l
 
 template <typename S, bool DO_RES, int NT>
 __global__ void __launch_bounds__(NT) k_sweep_finish(const BlockDev<S>* __restrict__ blocks,
-                                                     const Chunk* __restrict__ chunks, ParamsDev P,
+                                                     const Chunk* __restrict__ chunks, ParamsDev P_launch,
                                                      ResPartial* __restrict__ partials) {
   // Natural order (interior index n = i + ni*(j + nj*k)): prim, dq, vol, dt
   // and the mask are read and written coalesced; only the swept increment is
   // gathered from the plane-major layout, at c = koff[s*nk + k] + (j - jlo(s,k)).
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
+  const ParamsDev& P = block_params(B, P_launch);
   const long long np = B.npad, nc = B.ncomp;
   double sum = 0.0, mx = -1.0;
   long long key = (long long)0x7fffffffffffffffLL;
@@ -1865,9 +1896,10 @@ __device__ __forceinline__ void block_reduce_res(double& sum, double& mx, long l
 
 template <typename S, bool DO_UPDATE, bool DO_RES, int NT>
 __global__ void __launch_bounds__(NT) k_update_res(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks,
-                                                   ParamsDev P, ResPartial* __restrict__ partials) {
+                                                   ParamsDev P_launch, ResPartial* __restrict__ partials) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
+  const ParamsDev& P = block_params(B, P_launch);
   const long long np = B.npad;
   double sum = 0.0, mx = -1.0;
   long long key = (long long)0x7fffffffffffffffLL;
@@ -1910,11 +1942,44 @@ __global__ void __launch_bounds__(NT) k_update_res(const BlockDev<S>* __restrict
 }
 
 template <typename S>
+__device__ __forceinline__ void res_final_body(const BlockDev<S>* __restrict__ blocks, int nblocks,
+                                               const ResPartial* __restrict__ partials, int npart,
+                                               long long total_points, const unsigned long long* dtmin_bits,
+                                               ResidualOut* __restrict__ hist, int* __restrict__ counter,
+                                               int capacity, ResPartial* __restrict__ total);
+
+template <typename S>
 __global__ void __launch_bounds__(1024) k_res_final(const BlockDev<S>* __restrict__ blocks, int nblocks,
                                                      const ResPartial* __restrict__ partials, int npart,
                                                      long long total_points, const unsigned long long* dtmin_bits,
                                                      ResidualOut* __restrict__ hist, int* __restrict__ counter,
                                                      int capacity, ResPartial* __restrict__ total) {
+  res_final_body<S>(blocks, nblocks, partials, npart, total_points, dtmin_bits, hist, counter, capacity, total);
+}
+
+// One CTA per case of a group: that case's minimum time step (dt_part) or
+// residual statistics (partials) over its own range, in the same order as
+// the case's own launches, into the case's own result slots.
+static __global__ void __launch_bounds__(1024) k_dtmin_group(const GroupMember* __restrict__ members,
+                                                             const double* __restrict__ dt_part) {
+  const GroupMember& m = members[blockIdx.x];
+  dtmin_final_body(dt_part + m.pad_off, m.pad_n, m.dtmin);
+}
+
+template <typename S>
+__global__ void __launch_bounds__(1024) k_res_final_group(const GroupMember* __restrict__ members,
+                                                           const ResPartial* __restrict__ partials, int capacity) {
+  const GroupMember& m = members[blockIdx.x];
+  res_final_body<S>(static_cast<const BlockDev<S>*>(m.blocks), m.nblocks, partials + m.part_off, m.part_n,
+                    m.total_points, m.dtmin, m.hist, m.counter, capacity, m.total);
+}
+
+template <typename S>
+__device__ __forceinline__ void res_final_body(const BlockDev<S>* __restrict__ blocks, int nblocks,
+                                               const ResPartial* __restrict__ partials, int npart,
+                                               long long total_points, const unsigned long long* dtmin_bits,
+                                               ResidualOut* __restrict__ hist, int* __restrict__ counter,
+                                               int capacity, ResPartial* __restrict__ total) {
   double sum = 0.0, mx = -1.0;
   long long key = (long long)0x7fffffffffffffffLL;
   for (int t = threadIdx.x; t < npart; t += 1024) {
@@ -1962,9 +2027,10 @@ __device__ __forceinline__ double splitmix_uniform(unsigned long long seed, unsi
 
 template <typename S>
 __global__ void k_init_flow(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks,
-                            const long long* __restrict__ pad_base, ParamsDev P, unsigned long long seed, double amp) {
+                            const long long* __restrict__ pad_base, ParamsDev P_launch, unsigned long long seed, double amp) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
+  const ParamsDev& P = block_params(B, P_launch);
   const long long np = B.npad;
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
     const long long idx = ch.start + t;

@@ -127,6 +127,7 @@ void carve_block(char* base, const HostBlock& b, BlockDev<S>& d) {
   d.sk_pair = sk + 44 * nc;
   d.sk_gm = sk + 74 * nc;
   d.sk_inv = sk + 77 * nc;
+  d.params = nullptr;  // a case's own launches pass its parameters
   d.ni = b.idim;
   d.nj = b.jdim;
   d.nk = b.kdim;
@@ -278,6 +279,7 @@ int build_line_tiles(orion_case_t c) {
     if (lanes < 1) return fail(ORION_E_UNSUPPORTED, "grid line too long for the line kernels");
     if (d > 0 && lanes >= 8) lanes = lanes / 8 * 8;
     L.lanes[d] = lanes;
+    L.line_units[d] = lanes * (lmax + 1);
     std::vector<LineTile> tiles;
     for (int b = 0; b < nb; ++b) {
       const auto& h = c->hb[b];
@@ -290,14 +292,17 @@ int build_line_tiles(orion_case_t c) {
   return 0;
 }
 
-// Tile wavefront sweeps: tiles of 32 x kTileK grid lines, per direction in
-// ticket order.  A tile's start in steps is 32 J + kTileK K behind its
+// Tile wavefront sweeps: tiles of 32 x TK grid lines (TK per precision,
+// TileShape), per direction in ticket order.  A tile's start in steps is
+// 32 J + TK K behind its
 // block's first tile, and its upstream tiles (J-1, K) and (J, K-1) start
 // strictly earlier, so ordering by start offset (ties by block, then J) is a
 // dependency-respecting order for every block at once.
 int build_sweep_tiles(orion_case_t c) {
   auto& L = c->L;
-  constexpr int TJ = 32, TK = kTileK;
+  constexpr int TJ = 32;
+  const int TK = c->prec == ORION_PREC_FP64 ? TileShape<double>::TK : TileShape<float>::TK;
+  L.tile_k = TK;
   int maxn = 0;
   for (int dir = 0; dir < 2; ++dir) {
     struct Item {
@@ -867,6 +872,7 @@ int orion_case_create_shard(int nblocks, const orion_block_desc_t* blocks, const
 
 int orion_case_destroy(orion_case_t c) {
   if (!c) return 0;
+  if (c->group) return fail(ORION_E_INVALID, "the case belongs to a group: destroy the group first");
   cudaStreamSynchronize(c->stream);
   destroy_case(c);
   return 0;
@@ -941,6 +947,7 @@ int orion_case_get_schedule(orion_case_t c, orion_schedule_t* s) {
 
 static int launch_steps(orion_case_t c, int nsteps);
 static int sweep_status(orion_case_t c);
+static int enqueue_hist_copy(orion_case_t c, int nsteps);
 
 int orion_case_autotune(orion_case_t c, int steps_per_trial, orion_schedule_t* trials, int cap, int* ntrials,
                         orion_schedule_t* best) {
@@ -1076,7 +1083,7 @@ int orion_case_sweep_schedule(orion_case_t c, int out[5]) {
   out[0] = L.tiles_on ? 3 : (L.cl_size > 0 ? 2 : (L.persist_grid > 0 ? 1 : 0));
   out[1] = L.tiles_on ? L.n_sweep_tiles[0] : (L.cl_size > 0 ? L.cl_count : L.persist_grid);
   out[2] = L.cl_size;
-  out[3] = L.tiles_on ? 32 * kTileK : L.sweep_nt;
+  out[3] = L.tiles_on ? 32 * L.tile_k : L.sweep_nt;
   out[4] = L.max_planes;
   return 0;
 }
@@ -1345,6 +1352,12 @@ int orion_step_submit(orion_case_t c, int nsteps) {
   if (nsteps == 0) return 0;
   int rc = launch_steps(c, nsteps);
   if (rc) return rc;
+  return enqueue_hist_copy(c, nsteps);
+}
+
+// Copies the history entries of the last nsteps steps (enqueued on the case's
+// stream) into the case's pinned ring and records them as pending.
+static int enqueue_hist_copy(orion_case_t c, int nsteps) {
   // the new entries sit at ring positions [first, first + nsteps) mod kHistCap
   const long long first = c->hist_count;
   long long pos = first % kHistCap;
@@ -1371,7 +1384,7 @@ int orion_case_poll(orion_case_t c, orion_residual_t* out, int cap, int* n) {
     cudaGetLastError();
     return fail(ORION_E_CUDA, std::string("case stream: ") + cudaGetErrorString(q));
   }
-  int rc = sweep_status(c);
+  int rc = sweep_status(c->group ? c->group->proxy : c);
   if (rc) return rc;
   const int take = std::min(cap, c->pending_n);
   for (int s = 0; s < take; ++s) {
@@ -1395,6 +1408,345 @@ int orion_last_residual(orion_case_t c, orion_residual_t* out) {
   CUDA_TRY(cudaMemcpy(&cnt, c->L.counter, sizeof(int), cudaMemcpyDeviceToHost));
   if (cnt <= 0) return fail(ORION_E_INVALID, "no step has run");
   return read_hist(c, cnt - 1, 1, out);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Groups: several cases stepped together, one launch per stage over the blocks
+// of every member.  The group's lists are the members' lists concatenated,
+// with block indices (and tile slots, pack slots, partial ranges) shifted by
+// the members before; every member keeps its own chunks, tiles and reduction
+// order, so its results are the same as when it steps alone.
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+int download(std::vector<T>& v, const T* d, size_t n) {
+  v.resize(n);
+  if (n) CUDA_TRY(cudaMemcpy(v.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+template <typename S>
+std::vector<BlockDev<S>>& host_blocks(orion_case_t c);
+template <>
+std::vector<BlockDev<double>>& host_blocks<double>(orion_case_t c) { return c->bd64; }
+template <>
+std::vector<BlockDev<float>>& host_blocks<float>(orion_case_t c) { return c->bd32; }
+
+template <typename S>
+int build_group(orion_group_t g, orion_case_t px) {
+  auto& L = px->L;
+  auto& mem = g->members;
+  const int nm = (int)mem.size();
+  int rc;
+  // block descriptors: the members' own, each pointing at its case's parameters
+  std::vector<BlockDev<S>> blocks;
+  std::vector<int> boff(nm + 1, 0);
+  ParamsDev* d_params = nullptr;
+  if ((rc = dev_alloc(px, &d_params, (size_t)nm))) return rc;
+  for (int m = 0; m < nm; ++m) {
+    CUDA_TRY(cudaMemcpyAsync(d_params + m, &mem[m]->P, sizeof(ParamsDev), cudaMemcpyHostToDevice, px->stream));
+    for (auto b : host_blocks<S>(mem[m])) {
+      b.params = d_params + m;
+      blocks.push_back(b);
+    }
+    boff[m + 1] = (int)blocks.size();
+  }
+  BlockDev<S>* d_blocks = nullptr;
+  CUDA_TRY(cudaMallocAsync((void**)&d_blocks, sizeof(BlockDev<S>) * blocks.size(), px->stream));
+  px->d_blocks = d_blocks;  // freed with the proxy
+  CUDA_TRY(cudaMemcpyAsync(d_blocks, blocks.data(), sizeof(BlockDev<S>) * blocks.size(), cudaMemcpyHostToDevice,
+                           px->stream));
+  px->nblocks = (int)blocks.size();
+
+  std::vector<GroupMember> gm(nm);
+  std::vector<Chunk> pad, itr;
+  std::vector<LineTile> tl[3];
+  std::vector<unsigned long long> hsrc, hdst;
+  std::vector<RegionDev> regs;
+  std::vector<std::vector<int>> phases;
+  std::vector<int> pk_block, ap_block, ap_off{0}, ap_slot;
+  std::vector<long long> pk_idx, ap_idx;
+  std::vector<std::vector<Chunk>> planes[2];
+  std::vector<SweepTile> stiles[2];
+  int max_planes = 0;
+  for (int m = 0; m < nm; ++m) {
+    orion_case_t c = mem[m];
+    const auto& M = c->L;
+    const int bo = boff[m];
+    std::vector<Chunk> v;
+    // padded and interior chunks; the member's partial ranges
+    if ((rc = download(v, M.pad_chunks, M.n_pad_chunks))) return rc;
+    gm[m].pad_off = (int)pad.size();
+    gm[m].pad_n = M.n_pad_chunks;
+    for (auto ch : v) { ch.block += bo; pad.push_back(ch); }
+    if ((rc = download(v, M.int_chunks, M.n_int_chunks))) return rc;
+    gm[m].part_off = (int)itr.size();
+    gm[m].part_n = M.n_int_chunks;
+    for (auto ch : v) { ch.block += bo; itr.push_back(ch); }
+    gm[m].blocks = d_blocks + bo;
+    gm[m].nblocks = c->nblocks;
+    gm[m].total_points = c->total_interior * 5;
+    gm[m].dtmin = M.dtmin;
+    gm[m].hist = M.hist;
+    gm[m].counter = M.counter;
+    gm[m].total = M.res_total;
+    // line tiles
+    for (int d = 0; d < 3; ++d) {
+      std::vector<LineTile> t;
+      if ((rc = download(t, M.tiles[d], M.n_tiles[d]))) return rc;
+      for (auto x : t) { x.block += bo; tl[d].push_back(x); }
+      L.lanes[d] = std::max(L.lanes[d], M.lanes[d]);
+      L.lmax[d] = std::max(L.lmax[d], M.lmax[d]);
+      L.line_units[d] = std::max(L.line_units[d], M.line_units[d]);
+    }
+    // halo copy as element addresses
+    {
+      std::vector<long long> a, b;
+      if ((rc = download(a, M.halo_src, M.n_halo)) || (rc = download(b, M.halo_dst, M.n_halo))) return rc;
+      const unsigned long long base = (unsigned long long)(uintptr_t)c->arena;
+      for (int q = 0; q < M.n_halo; ++q) {
+        hsrc.push_back(base + 8ull * (unsigned long long)a[q]);
+        hdst.push_back(base + 8ull * (unsigned long long)b[q]);
+      }
+    }
+    // physical BC phases: the p-th region of every block of every member
+    {
+      std::vector<RegionDev> r;
+      std::vector<int> pl;
+      const int nreg = M.phase_off.empty() ? 0 : M.phase_off.back();
+      if ((rc = download(pl, M.phase_regions, (size_t)nreg))) return rc;
+      int maxr = 0;
+      for (int x : pl) maxr = std::max(maxr, x + 1);
+      if ((rc = download(r, M.regions, (size_t)maxr))) return rc;
+      const int rbase = (int)regs.size();
+      for (auto x : r) { x.block += bo; regs.push_back(x); }
+      for (size_t p = 0; p + 1 < M.phase_off.size(); ++p) {
+        if (phases.size() <= p) phases.resize(p + 1);
+        for (int q = M.phase_off[p]; q < M.phase_off[p + 1]; ++q) phases[p].push_back(rbase + pl[q]);
+      }
+    }
+    // interface averaging: own slots packed in member order
+    {
+      std::vector<int> pb, ab, ao, as;
+      std::vector<long long> pi, ai;
+      if ((rc = download(pb, M.pk_block, M.n_pack)) || (rc = download(pi, M.pk_idx, M.n_pack))) return rc;
+      if ((rc = download(ab, M.ap_block, M.n_ap)) || (rc = download(ai, M.ap_idx, M.n_ap))) return rc;
+      if ((rc = download(ao, M.ap_off, M.n_ap ? (size_t)M.n_ap + 1 : 0))) return rc;
+      if ((rc = download(as, M.ap_slot, M.n_ap ? (size_t)ao.back() : 0))) return rc;
+      const int slot_base = (int)pk_block.size(), ent_base = (int)ap_slot.size();
+      for (int q = 0; q < M.n_pack; ++q) { pk_block.push_back(pb[q] + bo); pk_idx.push_back(pi[q]); }
+      for (int q = 0; q < M.n_ap; ++q) {
+        ap_block.push_back(ab[q] + bo);
+        ap_idx.push_back(ai[q]);
+        ap_off.push_back(ent_base + ao[q + 1]);
+      }
+      for (int x : as) {
+        if (x >= M.n_pack) return fail(ORION_E_UNSUPPORTED, "a shard cannot join a group");
+        ap_slot.push_back(slot_base + x);
+      }
+    }
+    // sweeps: hyperplane t of every member, or the members' tiles after one another
+    for (int dir = 0; dir < 2; ++dir) {
+      const auto& off = M.sweep_off[dir];
+      if (!off.empty()) {
+        std::vector<Chunk> ch;
+        if ((rc = download(ch, M.sweep_chunks[dir], (size_t)off.back()))) return rc;
+        const int np = (int)off.size() - 1;
+        if ((int)planes[dir].size() < np) planes[dir].resize(np);
+        for (int t = 0; t < np; ++t)
+          for (int q = off[t]; q < off[t + 1]; ++q) {
+            Chunk x = ch[q];
+            x.block += bo;
+            planes[dir][t].push_back(x);
+          }
+      }
+      std::vector<SweepTile> st;
+      if ((rc = download(st, static_cast<const SweepTile*>(M.sweep_tiles[dir]), (size_t)M.n_sweep_tiles[dir])))
+        return rc;
+      const int sb = (int)stiles[dir].size();
+      for (auto x : st) {
+        x.block += bo;
+        if (x.up_j >= 0) x.up_j += sb;
+        if (x.up_k >= 0) x.up_k += sb;
+        stiles[dir].push_back(x);
+      }
+    }
+    max_planes = std::max(max_planes, M.max_planes);
+  }
+  // upload
+  if ((rc = dev_upload(px, &L.pad_chunks, pad))) return rc;
+  L.n_pad_chunks = (int)pad.size();
+  if ((rc = dev_upload(px, &L.int_chunks, itr))) return rc;
+  L.n_int_chunks = (int)itr.size();
+  for (int d = 0; d < 3; ++d) {
+    if ((rc = dev_upload(px, &L.tiles[d], tl[d]))) return rc;
+    L.n_tiles[d] = (int)tl[d].size();
+  }
+  GroupRun& G = g->run;
+  if ((rc = dev_upload(px, &G.halo_src, hsrc)) || (rc = dev_upload(px, &G.halo_dst, hdst))) return rc;
+  G.n_halo = (int)hsrc.size();
+  {
+    std::vector<int> plist;
+    L.phase_off.assign(1, 0);
+    L.phase_maxpts.clear();
+    for (auto& ph : phases) {
+      int mx = 0;
+      for (int r : ph) {
+        plist.push_back(r);
+        mx = std::max(mx, regs[r].npts);
+      }
+      L.phase_off.push_back((int)plist.size());
+      L.phase_maxpts.push_back(mx);
+    }
+    if ((rc = dev_upload(px, &L.regions, regs)) || (rc = dev_upload(px, &L.phase_regions, plist))) return rc;
+  }
+  if ((rc = dev_upload(px, &L.pk_block, pk_block)) || (rc = dev_upload(px, &L.pk_idx, pk_idx))) return rc;
+  L.n_pack = (int)pk_block.size();
+  if ((rc = dev_alloc(px, &L.pack, (size_t)std::max(L.n_pack, 1) * 5))) return rc;
+  if ((rc = dev_upload(px, &L.ap_block, ap_block)) || (rc = dev_upload(px, &L.ap_idx, ap_idx))) return rc;
+  if ((rc = dev_upload(px, &L.ap_off, ap_off)) || (rc = dev_upload(px, &L.ap_slot, ap_slot))) return rc;
+  L.n_ap = (int)ap_block.size();
+  L.max_planes = max_planes;
+  for (int dir = 0; dir < 2; ++dir) {
+    std::vector<Chunk> ch;
+    std::vector<int> off{0};
+    for (auto& v : planes[dir]) {
+      ch.insert(ch.end(), v.begin(), v.end());
+      off.push_back((int)ch.size());
+    }
+    if ((rc = dev_upload(px, &L.sweep_chunks[dir], ch))) return rc;
+    L.sweep_off[dir] = off;
+    SweepTile* d = nullptr;
+    if ((rc = dev_upload(px, &d, stiles[dir]))) return rc;
+    L.sweep_tiles[dir] = d;
+    L.n_sweep_tiles[dir] = (int)stiles[dir].size();
+  }
+  L.sweep_nt = kSweepThreads;
+  {
+    const int mx = std::max(L.n_sweep_tiles[0], L.n_sweep_tiles[1]);
+    unsigned char* ctl = nullptr;
+    if ((rc = dev_alloc(px, &ctl, offsetof(TileCtl, progress) + sizeof(unsigned int) * (size_t)std::max(mx, 1))))
+      return rc;
+    L.tile_ctl = ctl;
+    L.tile_k = mem[0]->L.tile_k;
+    int* sctl = nullptr;
+    if ((rc = dev_alloc(px, &sctl, 4))) return rc;
+    L.sweep_ctl = sctl;
+  }
+  if ((rc = dev_alloc(px, &L.partials, (size_t)std::max(L.n_int_chunks, 1)))) return rc;
+  if ((rc = dev_alloc(px, &L.dt_part, (size_t)std::max(L.n_pad_chunks, 1)))) return rc;
+  if ((rc = dev_upload(px, &G.members, gm))) return rc;
+  G.nmembers = nm;
+  L.group = &G;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int orion_group_create(int n, const orion_case_t* cases, orion_group_t* out) {
+  if (n < 1 || !cases || !out) return fail(ORION_E_INVALID, "bad arguments");
+  *out = nullptr;
+  for (int m = 0; m < n; ++m) {
+    const orion_case_t c = cases[m];
+    if (!c) return fail(ORION_E_INVALID, "null case");
+    if (c->prec != cases[0]->prec) return fail(ORION_E_UNSUPPORTED, "the cases of a group share one precision");
+    if (c->P.nvis != cases[0]->P.nvis) return fail(ORION_E_UNSUPPORTED, "the cases of a group are all viscous or all Euler");
+    if (c->shard.nranks > 1) return fail(ORION_E_UNSUPPORTED, "a shard cannot join a group");
+    if (c->pending_n > 0) return fail(ORION_E_INVALID, "a case has submitted steps that have not been polled");
+    if (c->group) return fail(ORION_E_INVALID, "a case belongs to another group");
+    for (int q = 0; q < m; ++q)
+      if (cases[q] == c) return fail(ORION_E_INVALID, "a case is listed twice");
+  }
+  std::lock_guard<std::mutex> lk(g_struct_mu);
+  auto g = std::make_unique<orion_group_s>();
+  g->members.assign(cases, cases + n);
+  auto px = std::make_unique<orion_case_s>();
+  px->prec = cases[0]->prec;
+  px->P = cases[0]->P;  // not read: every block carries its case's parameters
+  px->device = cases[0]->device;
+  CUDA_TRY(cudaSetDevice(px->device));
+  CUDA_TRY(cudaStreamCreateWithFlags(&px->stream, cudaStreamNonBlocking));
+  px->own_stream = true;
+  bool tiles = true;
+  for (auto c : g->members) {
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    tiles = tiles && c->L.tiles_on;
+  }
+  px->L.tiles_on = tiles;  // otherwise one launch per hyperplane
+  g->proxy = px.get();
+  int rc = px->prec == ORION_PREC_FP64 ? build_group<double>(g.get(), px.get()) : build_group<float>(g.get(), px.get());
+  if (!rc) rc = ops_for(px->prec).set_attributes();
+  if (!rc) {
+    cudaError_t e = cudaStreamSynchronize(px->stream);
+    if (e != cudaSuccess) rc = fail(ORION_E_CUDA, std::string("group set-up: ") + cudaGetErrorString(e));
+  }
+  if (rc) {
+    destroy_case(px.release());
+    return rc;
+  }
+  for (auto c : g->members) {
+    g->saved_streams.push_back(c->stream);
+    c->stream = px->stream;  // the members' copies, polls and per-stage calls follow the group's launches
+    c->group = g.get();
+  }
+  px.release();
+  *out = g.release();
+  return 0;
+}
+
+int orion_group_destroy(orion_group_t g) {
+  if (!g) return 0;
+  std::lock_guard<std::mutex> lk(g_struct_mu);
+  cudaStreamSynchronize(g->proxy->stream);
+  for (size_t m = 0; m < g->members.size(); ++m) {
+    g->members[m]->stream = g->saved_streams[m];
+    g->members[m]->group = nullptr;
+  }
+  destroy_case(g->proxy);
+  delete g;
+  return 0;
+}
+
+int orion_group_submit(orion_group_t g, int nsteps) {
+  if (!g || nsteps < 0) return fail(ORION_E_INVALID, "bad arguments");
+  for (auto c : g->members) {
+    if (c->pending_n + nsteps > kHistCap)
+      return fail(ORION_E_INVALID, "more unpolled steps than the history ring holds (4096)");
+    if (!c->hist_host && !(c->hist_host = acquire_hist_ring())) return fail(ORION_E_NOMEM, "pinned history ring");
+    if (c->hist_count < 0) {
+      int cnt = 0;
+      CUDA_TRY(cudaStreamSynchronize(c->stream));
+      CUDA_TRY(cudaMemcpy(&cnt, c->L.counter, sizeof(int), cudaMemcpyDeviceToHost));
+      c->hist_count = cnt;
+    }
+  }
+  if (nsteps == 0) return 0;
+  int rc = launch_steps(g->proxy, nsteps);
+  if (rc) return rc;
+  for (auto c : g->members) {
+    c->steps_done += nsteps;
+    if ((rc = enqueue_hist_copy(c, nsteps))) return rc;
+  }
+  return 0;
+}
+
+int orion_group_sync(orion_group_t g) {
+  if (!g) return fail(ORION_E_INVALID, "null group");
+  CUDA_TRY(cudaStreamSynchronize(g->proxy->stream));
+  return sweep_status(g->proxy);
+}
+
+int orion_group_step_launches(orion_group_t g, int* n) {
+  if (!g || !n) return fail(ORION_E_INVALID, "null argument");
+  int rc = ensure_graph(g->proxy);
+  if (rc) return rc;
+  *n = g->proxy->step_launches;
+  return 0;
 }
 
 // ---------------------------------------------------------------------------

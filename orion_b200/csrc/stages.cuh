@@ -26,14 +26,17 @@ struct Stages {
     return rc;
   }
 
+  // dynamic shared memory the tile sweeps may ask for (prefetch buffers and
+  // the row-base cache of blocks of up to about 2,500 hyperplanes)
+  static constexpr size_t kTileSmemMax = 160 * 1024;
+
   static int set_line_attributes() {
     const int b = (int)kLineSmemBudget;
-    CUDA_TRY(cudaFuncSetAttribute(k_sweep_tiles<S, T, SW_LUSGS_FWD, 1, kTileK>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-    CUDA_TRY(cudaFuncSetAttribute(k_sweep_tiles<S, T, SW_LUSGS_BWD, -1, kTileK>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-    CUDA_TRY(cudaFuncSetAttribute(k_sweep_tiles<S, T, SW_GS, 1, kTileK>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-    CUDA_TRY(cudaFuncSetAttribute(k_sweep_tiles<S, T, SW_GS, -1, kTileK>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    const int tb = (int)kTileSmemMax;
+    CUDA_TRY(cudaFuncSetAttribute(k_sweep_tiles<S, T, SW_LUSGS_FWD, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tb));
+    CUDA_TRY(cudaFuncSetAttribute(k_sweep_tiles<S, T, SW_LUSGS_BWD, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tb));
+    CUDA_TRY(cudaFuncSetAttribute(k_sweep_tiles<S, T, SW_GS, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tb));
+    CUDA_TRY(cudaFuncSetAttribute(k_sweep_tiles<S, T, SW_GS, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tb));
     CUDA_TRY(cudaFuncSetAttribute(k_viscous<0, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
     CUDA_TRY(cudaFuncSetAttribute(k_viscous<1, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
     CUDA_TRY(cudaFuncSetAttribute(k_viscous<2, S, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
@@ -45,6 +48,13 @@ struct Stages {
 
   static int exchange(orion_case_t c) {
     auto& L = c->L;
+    if (L.group) {
+      const GroupRun& G = *L.group;
+      if (G.n_halo > 0)
+        k_halo_copy_abs<<<(G.n_halo + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(G.halo_src, G.halo_dst,
+                                                                                          G.n_halo);
+      return 0;
+    }
     if (L.n_halo > 0)
       k_halo_copy<<<(L.n_halo + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(
           static_cast<double*>(c->arena), L.halo_src, L.halo_dst, L.n_halo);
@@ -72,7 +82,12 @@ struct Stages {
       k_state<S, true, false><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dt_part);
     else
       k_state<S, false, false><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dt_part);
-    if (with_dt) k_dtmin_final<<<1, 1024, 0, c->stream>>>(L.dt_part, L.n_pad_chunks, L.dtmin);
+    if (with_dt) {
+      if (L.group)
+        k_dtmin_group<<<L.group->nmembers, 1024, 0, c->stream>>>(L.group->members, L.dt_part);
+      else
+        k_dtmin_final<<<1, 1024, 0, c->stream>>>(L.dt_part, L.n_pad_chunks, L.dtmin);
+    }
     return 0;
   }
 
@@ -86,7 +101,7 @@ struct Stages {
   template <int D>
   static void visc_dir(orion_case_t c) {
     auto& L = c->L;
-    const size_t smem = (size_t)L.lanes[D] * (L.lmax[D] + 1) * 4 * sizeof(T);
+    const size_t smem = (size_t)L.line_units[D] * 4 * sizeof(T);
     k_viscous<D, S, T><<<L.n_tiles[D], kThreads, smem, c->stream>>>(blocks(c), L.tiles[D], c->P);
   }
 
@@ -103,7 +118,7 @@ struct Stages {
   template <int D>
   static void inv_dir(orion_case_t c) {
     auto& L = c->L;
-    const size_t smem = (size_t)L.lanes[D] * (L.lmax[D] + 1) * 5 * sizeof(T);
+    const size_t smem = (size_t)L.line_units[D] * 5 * sizeof(T);
     k_inviscid<D, S, T><<<L.n_tiles[D], kThreads, smem, c->stream>>>(blocks(c), L.tiles[D], c->P);
   }
 
@@ -336,7 +351,9 @@ struct Stages {
     CUDA_TRY(cudaMemsetAsync(L.tile_ctl, 0, offsetof(TileCtl, progress) + sizeof(unsigned int) * (size_t)n,
                              c->stream));
     SweepCtl* sc = static_cast<SweepCtl*>(L.sweep_ctl);
-    k_sweep_tiles<S, T, MODE, DIR, kTileK><<<n, 32 * kTileK + 32, tile_ring_bytes<T, MODE, kTileK>(), c->stream>>>(
+    const size_t smem = tile_smem_bytes<T, MODE>(L.max_planes);
+    if (smem > kTileSmemMax) return fail(ORION_E_UNSUPPORTED, "block too long for the tile sweeps' row-base cache");
+    k_sweep_tiles<S, T, MODE, DIR><<<n, 32 * TileShape<T>::TK + 32, smem, c->stream>>>(
         blocks(c), static_cast<const SweepTile*>(L.sweep_tiles[d]), n, static_cast<TileCtl*>(L.tile_ctl),
         &sc->error, c->P, L.spin_limit);
     return 0;
@@ -395,6 +412,10 @@ struct Stages {
 
   static void residual_final(orion_case_t c) {
     auto& L = c->L;
+    if (L.group) {
+      k_res_final_group<S><<<L.group->nmembers, 1024, 0, c->stream>>>(L.group->members, L.partials, kHistCap);
+      return;
+    }
     k_res_final<S><<<1, 1024, 0, c->stream>>>(blocks(c), c->nblocks, L.partials, L.n_int_chunks, c->total_interior * 5,
                                               L.dtmin, L.hist, L.counter, kHistCap, L.res_total);
   }

@@ -98,16 +98,62 @@ __device__ __forceinline__ long long row_base(const int* __restrict__ koff, int 
 // Bound of a compute warp's wait for the control warp (about four seconds).
 constexpr long long kComputeWaitCycles = 8000000000LL;
 
-// Dynamic shared memory of one tile CTA: the 4-slot ring of neighbour-visible
-// state (8 values per point, 13 on the GS passes).
-template <typename T, int MODE, int TK>
-constexpr size_t tile_ring_bytes() {
-  return (size_t)4 * (MODE == SW_GS ? 13 : 8) * TK * 32 * sizeof(T);
-}
-
 __device__ __forceinline__ void compute_barrier(int nthreads) {
   asm volatile("bar.sync 1, %0;\n" ::"r"(nthreads) : "memory");
 }
+
+// Prefetch distance (steps) and tile height of each precision: FP32 tiles are
+// 32 x 4 lines and read their operands three steps ahead, FP64 tiles 32 x 2
+// lines two steps ahead (the prefetch buffers live in shared memory).
+#ifndef ORION_TILE_K_F32
+#define ORION_TILE_K_F32 4
+#endif
+#ifndef ORION_TILE_PD_F32
+#define ORION_TILE_PD_F32 3
+#endif
+#ifndef ORION_TILE_K_F64
+#define ORION_TILE_K_F64 2
+#endif
+#ifndef ORION_TILE_PD_F64
+#define ORION_TILE_PD_F64 2
+#endif
+template <typename T> struct TileShape;
+template <> struct TileShape<float> { static constexpr int TK = ORION_TILE_K_F32, PD = ORION_TILE_PD_F32; };
+template <> struct TileShape<double> { static constexpr int TK = ORION_TILE_K_F64, PD = ORION_TILE_PD_F64; };
+
+// Fields a point's owner prefetches: static operands (coed, own: rhs or the
+// forward increment, metrics 9, |grad| 3, 1/|grad| 3) for itself, and the
+// neighbour-visible state (u, v, w, H, c^2, af, c, viscous factor, and on the
+// GS passes the old increment) for the adjacent threads.
+constexpr int kTileStatics = 21;
+template <int MODE> __host__ __device__ constexpr int tile_ring_fields() { return MODE == SW_GS ? 13 : 8; }
+
+// Dynamic shared memory of one tile CTA with `npl` hyperplanes at most.
+// Edge records: the state (8) and increment (5) of a neighbour in another
+// tile, per step slot, for the first and last lane of every k row (j edges)
+// and every lane of the first and last k row (k edges).
+constexpr int kTileEdgeFields = 13;
+template <int TK> __host__ __device__ constexpr int tile_edge_records() { return 2 * TK + 64; }
+
+template <typename T, int MODE>
+constexpr size_t tile_smem_bytes(int npl) {
+  constexpr int TK = TileShape<T>::TK, PD = TileShape<T>::PD;
+  return (size_t)((PD + 1) * kTileStatics + (PD + 2) * tile_ring_fields<MODE>()) * TK * 32 * sizeof(T) +
+         (size_t)(PD + 1) * tile_edge_records<TK>() * kTileEdgeFields * sizeof(T) +
+         (size_t)(TK + 2) * npl * sizeof(int);
+}
+
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+  const unsigned int s = (unsigned int)__cvta_generic_to_shared(smem);
+  if (sizeof(T) == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // MODE: SW_LUSGS_FWD (forward, behind = lower, uses q 0..2), SW_LUSGS_BWD
 // (backward, behind = upper, uses q 3..5), SW_GS with DIR +1 / -1 (all six).
@@ -121,12 +167,26 @@ __device__ __forceinline__ void compute_barrier(int nthreads) {
 // wait gives up, the control warp raises the error word and releases every
 // remaining step: the compute warps finish the tile on whatever data is there
 // (every access stays in bounds) and the host reports ORION_E_TIMEOUT.
-template <typename S, typename T, int MODE, int DIR, int TK>
-__global__ void __launch_bounds__(32 * TK + 32) k_sweep_tiles(const BlockDev<S>* __restrict__ blocks,
-                                                              const SweepTile* __restrict__ tiles, int ntiles,
-                                                              TileCtl* __restrict__ ctl, int* __restrict__ err,
-                                                              ParamsDev P, long long spin_limit) {
-  constexpr int TJ = 32;
+//
+// Each compute thread copies its own points' operands PD steps ahead with
+// cp.async into shared memory: the static operands into a (PD+1)-slot buffer
+// of its own, the neighbour-visible state into a (PD+2)-slot ring the adjacent
+// threads read at step t from slot t-1 (behind neighbours) and t+1 (ahead).
+// New increments of the behind neighbours come from the previous step
+// (registers for i, s_dq for j and k).  Neighbours in other tiles are
+// prefetched with the same lead into per-step edge records; a step's operands
+// are fetched only once the upstream tiles allow that step, so the compute of
+// a step never waits on memory.  The row bases of the tile's k rows (and the
+// rows on either side) are cached in shared memory for every hyperplane.
+template <typename S, typename T, int MODE, int DIR>
+__global__ void __launch_bounds__(32 * TileShape<T>::TK + 32) k_sweep_tiles(const BlockDev<S>* __restrict__ blocks,
+                                                                           const SweepTile* __restrict__ tiles,
+                                                                           int ntiles, TileCtl* __restrict__ ctl,
+                                                                           int* __restrict__ err, ParamsDev P_launch,
+                                                                           long long spin_limit) {
+  static_assert(sizeof(S) == sizeof(T), "the tile sweeps keep operands in their storage precision");
+  constexpr int TJ = 32, TK = TileShape<T>::TK, PD = TileShape<T>::PD;
+  constexpr int NSS = PD + 1, NSR = PD + 2, NR = tile_ring_fields<MODE>(), NS = kTileStatics;
   constexpr int Q0 = MODE == SW_LUSGS_BWD ? 3 : 0;
   constexpr int Q1 = MODE == SW_LUSGS_FWD ? 3 : 6;
   // behind neighbours (updated in this pass) are q = QB .. QB+2
@@ -146,6 +206,7 @@ __global__ void __launch_bounds__(32 * TK + 32) k_sweep_tiles(const BlockDev<S>*
   if (slot >= ntiles) return;
   const SweepTile W = tiles[slot];
   const BlockDev<S>& Bd = blocks[W.block];
+  const ParamsDev& P = block_params(Bd, P_launch);
   const int ni = Bd.ni;
   const int nsteps = ni + TJ + TK - 2;
 
@@ -192,21 +253,14 @@ __global__ void __launch_bounds__(32 * TK + 32) k_sweep_tiles(const BlockDev<S>*
   }
 
   // ---------------- compute warps ----------------
-  // Each thread prefetches its own coming points only: the static operands of
-  // its next point (registers) and the neighbour-visible state (u, v, w, H,
-  // c^2, af, c, viscous factor; on the GS passes also the old increment) of
-  // the point after that, which it writes to a 4-slot ring in shared memory.
-  // At step t a point finds its in-tile neighbours' state in slot t-1
-  // (behind) and t+1 (ahead), their new increments in s_dq; only neighbours
-  // in other tiles are read from global memory.
-  constexpr int NR = MODE == SW_GS ? 13 : 8;  // ring fields per point
-  constexpr bool PF_STATIC = sizeof(T) == 4;   // FP32: prefetch the static operands a step ahead too
-  // dynamic shared memory: tile_ring_bytes<T, MODE, TK>()
   extern __shared__ __align__(16) unsigned char tile_smem[];
-  T(*s_ring)[NR][TK][TJ] = reinterpret_cast<T(*)[NR][TK][TJ]>(tile_smem);
+  T(*s_stat)[NS][TK][TJ] = reinterpret_cast<T(*)[NS][TK][TJ]>(tile_smem);
+  T(*s_ring)[NR][TK][TJ] = reinterpret_cast<T(*)[NR][TK][TJ]>(tile_smem + sizeof(T) * NSS * NS * TK * TJ);
+  constexpr int NE = tile_edge_records<TK>(), NEF = kTileEdgeFields;
+  T(*s_edge)[NE][NEF] = reinterpret_cast<T(*)[NE][NEF]>(tile_smem + sizeof(T) * (NSS * NS + NSR * NR) * TK * TJ);
+  int* s_rowb = reinterpret_cast<int*>(tile_smem + sizeof(T) * ((NSS * NS + NSR * NR) * TK * TJ + NSS * NE * NEF));
   const long long nc = Bd.ncomp;
-  const int nj = Bd.nj, nk = Bd.nk;
-  const int* const koff = Bd.koff;
+  const int nj = Bd.nj, nk = Bd.nk, npl = Bd.nplanes;
   S* const skdq = Bd.sk_dq;
   const S* const skcoed = Bd.sk_coed;
   const S* const skrhs = Bd.sk_rhs;
@@ -218,77 +272,129 @@ __global__ void __launch_bounds__(32 * TK + 32) k_sweep_tiles(const BlockDev<S>*
   const bool row = jj >= 0 && jj < nj && kk >= 0 && kk < nk;
   const T gm1 = T(P.gamma) - T(1);
   const int nvis = P.nvis;
+  // row bases of k rows kb - DIR .. kb + DIR*TK: compact index of (s, kk_r, jj) = s_rowb[r * npl + s] + jj
+  {
+    const int* const koff = Bd.koff;
+    for (int e = threadIdx.x; e < (TK + 2) * npl; e += 32 * TK) {
+      const int r = e / npl, sp = e - r * npl;
+      const int kr = W.kb + DIR * (r - 1);
+      s_rowb[e] = (kr >= 0 && kr < nk) ? (int)row_base(koff, ni, nk, sp, kr) : 0;
+    }
+  }
+  // rows of this thread (r = tk + 1) and its k neighbours (r = tk, tk + 2)
+  const int* const rb_own = s_rowb + (tk + 1) * npl;
+  const int* const rb_lo = s_rowb + (DIR > 0 ? tk : tk + 2) * npl;  // row kk - 1
+  const int* const rb_hi = s_rowb + (DIR > 0 ? tk + 2 : tk) * npl;  // row kk + 1
   auto valid = [&](int u) { return row && u >= 0 && u < ni; };
   auto ii_of = [&](int u) { return DIR > 0 ? u : ni - 1 - u; };
-  auto cidx = [&](int u) {  // compact index of this thread's point at sweep position u
-    const int ii = ii_of(u);
-    return row_base(koff, ni, nk, ii + jj + kk, kk) + jj;
-  };
-  // static operands: coed, own (rhs, or the forward increment on the backward
-  // LU-SGS pass), metrics 9, |grad| 3, 1/|grad| 3
-  constexpr int NS = 21;
-  auto load_static = [&](long long c, T v[NS]) {
-    v[0] = (T)skcoed[c];
-#pragma unroll
-    for (int m = 0; m < 5; ++m) v[1 + m] = MODE == SW_LUSGS_BWD ? (T)__ldcg(skdq + m * nc + c) : (T)skrhs[m * nc + c];
-#pragma unroll
-    for (int m = 0; m < 9; ++m) v[6 + m] = (T)skmet[m * nc + c];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      v[15 + d] = (T)skgm[d * nc + c];
-      v[18 + d] = (T)skinv[d * nc + c];
-    }
-  };
-  auto load_ring = [&](long long c, T v[NR]) {
-#pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = (T)sknbq[k * nc + c];
-    if (MODE == SW_GS) {
-#pragma unroll
-      for (int m = 0; m < 5; ++m) v[8 + m] = (T)__ldcg(skdq + m * nc + c);
-    }
-  };
-  auto store_ring = [&](int slot, const T v[NR]) {
-#pragma unroll
-    for (int k = 0; k < NR; ++k) s_ring[slot][k][tk][tj] = v[k];
-  };
+  compute_barrier(32 * TK);  // row bases ready
 
-  T st_cur[NS], st_next[NS], rg_next[NR];
-  // prologue: ring slots of steps 0 and 1, static operands of step 0
-  {
-    const int u0 = -tj - tk;
-    if (valid(u0)) {
-      load_ring(cidx(u0), rg_next);
-      store_ring(0, rg_next);
-    }
-    if (valid(u0 + 1)) {
-      load_ring(cidx(u0 + 1), rg_next);
-      store_ring(1, rg_next);
-    }
-    if (valid(u0)) load_static(cidx(u0), st_cur);
-  }
-  compute_barrier(32 * TK);
-
-  T prev[5] = {T(0), T(0), T(0), T(0), T(0)};  // this thread's increment of the previous step (behind-i)
-  for (int t = 0; t < nsteps; ++t) {
-    const int u = t - tj - tk;  // position along i in sweep order
-    // prefetch (independent of the upstream tiles: nobody else writes these)
-    const bool nxt1 = valid(u + 1), nxt2 = valid(u + 2);
-    if (PF_STATIC && nxt1) load_static(cidx(u + 1), st_next);
-    if (nxt2) load_ring(cidx(u + 2), rg_next);
-    if (*(volatile int*)&s_ready <= t) {  // bounded: the control warp releases or gives up well before this
+  // edge increments in flight: loaded at prefetch time, stored to the edge
+  // record at the end of the step
+  T edq[4][5];
+  T* edq_dst[4] = {nullptr, nullptr, nullptr, nullptr};
+  // waits (bounded) until the upstream tiles allow step x
+  auto wait_ready = [&](int x) {
+    if (*(volatile int*)&s_ready <= x) {  // bounded: the control warp releases or gives up well before this
       const long long t0 = clock64();
-      while (*(volatile int*)&s_ready <= t) {
+      while (*(volatile int*)&s_ready <= x) {
         if (clock64() - t0 > kComputeWaitCycles) {
           atomicExch(err, 1);
           break;
         }
       }
     }
+  };
+  // copies the operands of this thread's point at sweep position u into the
+  // buffers of step slot `step` (the upstream tiles must allow that step)
+  auto prefetch = [&](int u, int step) {
+    if (!valid(u)) return;
+    const int ii = ii_of(u);
+    const long long c = (long long)rb_own[ii + jj + kk] + jj;
+    T(*st)[TK][TJ] = s_stat[step % NSS];
+    T(*rg)[TK][TJ] = s_ring[step % NSR];
+    cp_async_elem(&st[0][tk][tj], skcoed + c);
+#pragma unroll
+    for (int m = 0; m < 5; ++m)
+      cp_async_elem(&st[1 + m][tk][tj], (MODE == SW_LUSGS_BWD ? (const S*)skdq : skrhs) + m * nc + c);
+#pragma unroll
+    for (int m = 0; m < 9; ++m) cp_async_elem(&st[6 + m][tk][tj], skmet + m * nc + c);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      cp_async_elem(&st[15 + d][tk][tj], skgm + d * nc + c);
+      cp_async_elem(&st[18 + d][tk][tj], skinv + d * nc + c);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) cp_async_elem(&rg[k][tk][tj], sknbq + k * nc + c);
+    if (MODE == SW_GS) {
+#pragma unroll
+      for (int m = 0; m < 5; ++m) cp_async_elem(&rg[8 + m][tk][tj], (const S*)skdq + m * nc + c);
+    }
+    // neighbours in other tiles: state by cp.async, increment (written during
+    // this pass by the upstream tile, or not yet by the downstream one) from
+    // L2 into registers, stored at the end of the step
+    const int s = ii + jj + kk;
+    T(*ed)[NEF] = s_edge[step % NSS];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      // e: 0 behind-j, 1 ahead-j, 2 behind-k, 3 ahead-k
+      const bool isj = e < 2, behind = (e & 1) == 0;
+      if (isj ? (behind ? tj != 0 : tj != TJ - 1) : (behind ? tk != 0 : tk != TK - 1)) continue;
+      if (MODE == SW_LUSGS_FWD && !behind) continue;  // these passes read behind neighbours only
+      if (MODE == SW_LUSGS_BWD && !behind) continue;
+      const bool lower = behind == (DIR > 0);  // natural lower neighbour (j-1 or k-1)
+      const int nd = isj ? jj + (lower ? -1 : 1) : kk + (lower ? -1 : 1);
+      if (nd < 0 || nd >= (isj ? nj : nk)) continue;
+      const int sn = lower ? s - 1 : s + 1;
+      const long long n = isj ? (long long)rb_own[sn] + nd : (long long)(lower ? rb_lo : rb_hi)[sn] + jj;
+      const int rec = isj ? (behind ? 0 : 1) * TK + tk : 2 * TK + (behind ? 0 : 1) * 32 + tj;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) cp_async_elem(&ed[rec][k], sknbq + k * nc + n);
+      T* const slotp = &ed[rec][8];
+#pragma unroll
+      for (int m = 0; m < 5; ++m) edq[e][m] = (T)__ldcg(skdq + m * nc + n);
+      edq_dst[e] = slotp;
+    }
+  };
+  auto store_edges = [&]() {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (!edq_dst[e]) continue;
+#pragma unroll
+      for (int m = 0; m < 5; ++m) edq_dst[e][m] = edq[e][m];
+      edq_dst[e] = nullptr;
+    }
+  };
+  {
+    const int u0 = -tj - tk;
+    wait_ready(min(PD, nsteps) - 1);
+#pragma unroll
+    for (int p = 0; p < PD; ++p) {
+      prefetch(u0 + p, p);
+      cp_async_commit();
+      store_edges();
+    }
+  }
+
+  T prev[5] = {T(0), T(0), T(0), T(0), T(0)};  // this thread's increment of the previous step (behind-i)
+  for (int t = 0; t < nsteps; ++t) {
+    cp_async_wait<PD - 2>();   // this thread's copies up to step t+1 have landed
+    compute_barrier(32 * TK);  // everybody's copies up to step t+1 and step t-1's increments are visible
+    if (threadIdx.x == 0 && t > 0) {
+      __threadfence_block();
+      *(volatile int*)&s_done = t;
+    }
+    const int u = t - tj - tk;  // position along i in sweep order
+    if (t + PD < nsteps) {
+      wait_ready(t + PD);
+      prefetch(u + PD, t + PD);
+    }
+    cp_async_commit();
     if (valid(u)) {
-      if (!PF_STATIC) load_static(cidx(u), st_cur);
+      const T(*st)[TK][TJ] = s_stat[t % NSS];
       const int ii = ii_of(u);
       const int s = ii + jj + kk;
-      const long long c = row_base(koff, ni, nk, s, kk) + jj;
+      const long long c = (long long)rb_own[s] + jj;
       bool has[6];
       has[0] = ii > 0;
       has[1] = jj > 0;
@@ -296,7 +402,9 @@ __global__ void __launch_bounds__(32 * TK + 32) k_sweep_tiles(const BlockDev<S>*
       has[3] = ii < ni - 1;
       has[4] = jj < nj - 1;
       has[5] = kk < nk - 1;
-      const int pb = (t - 1) & 1, rb = (t - 1) & 3, ra = (t + 1) & 3;
+      const int pb = (t - 1) & 1;
+      const T(*rgb)[TK][TJ] = s_ring[(t + NSR - 1) % NSR];
+      const T(*rga)[TK][TJ] = s_ring[(t + 1) % NSR];
       T rhs0[5] = {T(0), T(0), T(0), T(0), T(0)};
       // lower neighbours first (i, j, k), then upper (i, j, k): the reference's order
 #pragma unroll
@@ -311,9 +419,9 @@ __global__ void __launch_bounds__(32 * TK + 32) k_sweep_tiles(const BlockDev<S>*
         if (in_tile) {
           const int sj = d == 1 ? (behind ? tj - 1 : tj + 1) : tj;
           const int sk = d == 2 ? (behind ? tk - 1 : tk + 1) : tk;
-          const int slot = behind ? rb : ra;
+          const T(*rg)[TK][TJ] = behind ? rgb : rga;
 #pragma unroll
-          for (int k = 0; k < 8; ++k) nq[k] = s_ring[slot][k][sk][sj];
+          for (int k = 0; k < 8; ++k) nq[k] = rg[k][sk][sj];
           if (behind) {
             if (d == 0) {
 #pragma unroll
@@ -324,26 +432,24 @@ __global__ void __launch_bounds__(32 * TK + 32) k_sweep_tiles(const BlockDev<S>*
             }
           } else {
 #pragma unroll
-            for (int m = 0; m < 5; ++m) dn[m] = s_ring[slot][8 + m][sk][sj];
+            for (int m = 0; m < 5; ++m) dn[m] = rg[8 + m][sk][sj];
           }
         } else {
-          // neighbour in another tile: (ii, jj +- 1, kk) on plane s +- 1 or (ii, jj, kk +- 1)
-          const bool lower = q < 3;
-          const int sn = lower ? s - 1 : s + 1;
-          const long long n = d == 1 ? row_base(koff, ni, nk, sn, kk) + (lower ? jj - 1 : jj + 1)
-                                     : row_base(koff, ni, nk, sn, lower ? kk - 1 : kk + 1) + jj;
+          // neighbour in another tile: its record, prefetched with this step's operands
+          const int rec = d == 1 ? (behind ? 0 : 1) * TK + tk : 2 * TK + (behind ? 0 : 1) * 32 + tj;
+          const T* ed = s_edge[t % NSS][rec];
 #pragma unroll
-          for (int k = 0; k < 8; ++k) nq[k] = (T)sknbq[k * nc + n];
+          for (int k = 0; k < 8; ++k) nq[k] = ed[k];
 #pragma unroll
-          for (int m = 0; m < 5; ++m) dn[m] = (T)__ldcg(skdq + m * nc + n);
+          for (int m = 0; m < 5; ++m) dn[m] = ed[8 + m];
         }
         // the neighbour's state as seen through this point's metric: spectral
         // radius, split eigenvalues and viscous radius (calc_spectral_radius,
         // compute_flux_splitting, calc_visc_spectral_radius,
         // StateUpdater.cpp:175-265), in the reference's operation order
         T pc[5], nrm[3];
-        const T kx = st_cur[6 + 3 * d], ky = st_cur[7 + 3 * d], kz = st_cur[8 + 3 * d];
-        const T gmr = st_cur[15 + d], inv = st_cur[18 + d];
+        const T kx = st[6 + 3 * d][tk][tj], ky = st[7 + 3 * d][tk][tj], kz = st[8 + 3 * d][tk][tj];
+        const T gmr = st[15 + d][tk][tj], inv = st[18 + d][tk][tj];
         const T c2 = nq[4], cm = nq[6];
         const T ct = nq[0] * kx + nq[1] * ky + nq[2] * kz + T(0);
         const T r = tabs(ct) + cm * gmr;
@@ -365,10 +471,11 @@ __global__ void __launch_bounds__(32 * TK + 32) k_sweep_tiles(const BlockDev<S>*
         nrm[2] = kz * inv;
         split_term<T, MODE>(q, gm1, nvis, dn, nq, pc, nrm, rhs0);
       }
-      const T coed = st_cur[0];
+      const T coed = st[0][tk][tj];
 #pragma unroll
       for (int m = 0; m < 5; ++m) {
-        const T own = MODE == SW_LUSGS_BWD ? st_cur[1 + m] : -st_cur[1 + m];
+        const T ownv = st[1 + m][tk][tj];
+        const T own = MODE == SW_LUSGS_BWD ? ownv : -ownv;
         S v;
         if (MODE == SW_LUSGS_FWD) v = (S)((own + rhs0[m]) * coed);
         else if (MODE == SW_LUSGS_BWD) v = (S)(own - rhs0[m] * coed);
@@ -378,16 +485,13 @@ __global__ void __launch_bounds__(32 * TK + 32) k_sweep_tiles(const BlockDev<S>*
         prev[m] = (T)v;
       }
     }
-    if (nxt2) store_ring((t + 2) & 3, rg_next);
-    if (PF_STATIC && nxt1) {
-#pragma unroll
-      for (int k = 0; k < NS; ++k) st_cur[k] = st_next[k];
-    }
-    compute_barrier(32 * TK);  // step t's writes (shared and global) are done
-    if (threadIdx.x == 0) {
-      __threadfence_block();
-      *(volatile int*)&s_done = t + 1;
-    }
+    store_edges();
+  }
+  cp_async_wait<0>();
+  compute_barrier(32 * TK);
+  if (threadIdx.x == 0) {
+    __threadfence_block();
+    *(volatile int*)&s_done = nsteps;
   }
 }
 

@@ -6,16 +6,21 @@ free (admission by the case's device footprint, orion_footprint_estimate),
 builds its case (grid, metrics, initial state) on an admission thread while
 the GPU keeps running the admitted cases, and steps every admitted case on its
 own CUDA stream in quanta of graph-captured steps (orion_step_submit), so the
-work of all resident cases overlaps on the device.  A case retires at the end
+work of all resident cases overlaps on the device; by default (batched) every
+resident case is stepped in one group, one launch per stage over the blocks
+of all of them (orion_group_*), rebuilt between quanta when cases join or
+retire.  A case retires at the end
 of the first quantum in which its residual has dropped to `drop` times its
 first-step residual (rms, ResidualMonitor::compute), or after max_steps, or
 as diverged when its residual stops being finite or grows past diverge_growth
 (1e3) times the first step's; its memory is freed in stream order and the
 next request takes its place.
 
-Every case runs on its own stream with its own work lists and the same
-deterministic kernels whatever else is resident, and the quanta are the same,
-so a request's result does not depend on the mix it ran in.
+Every case keeps its own work lists and reductions and runs the same
+deterministic kernels whatever else is resident (alone, on its own stream, or
+in a group), and the quanta are the same, so a request's result does not
+depend on the mix it ran in.  A case steps whole quanta: max_steps should be a
+multiple of the quantum.
 
     python -m orion_b200.serving --requests 256 --mean-ms 50 --max-steps 2000
 """
@@ -131,7 +136,9 @@ class Server:
 
     def __init__(self, precision: int = _lib.PREC_MIXED, device: int = 0, hbm_budget: Optional[int] = None,
                  max_active: int = 256, quantum: int = 20, keep_state: bool = False, builders: int = 4,
-                 diverge_growth: float = 1e3, clock: Callable[[], float] = time.perf_counter):
+                 diverge_growth: float = 1e3, clock: Callable[[], float] = time.perf_counter,
+                 batched: bool = True):
+        self.batched = batched
         self.precision = precision
         self.device = device
         self.max_active = max_active
@@ -158,8 +165,116 @@ class Server:
 
         return solver.FlowFieldSet(req.build_case(), precision=self.precision, device=self.device)
 
+    def make_group(self, members: List[object]):
+        from . import solver
+
+        return solver.CaseGroup(members)
+
     # -- the loop ----------------------------------------------------------------------
     def run(self, requests: List[Request]) -> List[Result]:
+        if self.batched:
+            return self._run_batched(requests)
+        return self._run_streams(requests)
+
+    def _run_batched(self, requests: List[Request]) -> List[Result]:
+        """Every resident case in one group: one launch per stage for all of
+        them, `quantum` steps per round.  Between rounds the finished cases
+        retire, the cases built meanwhile join, and the group is rebuilt when
+        its membership changed."""
+        pending = deque(sorted(requests, key=lambda r: r.arrival_s))
+        queue: deque = deque()
+        active: Dict[int, _Slot] = {}
+        results: List[Result] = []
+        used = 0
+        building: List[tuple] = []  # (future, request, footprint), oldest first
+        ready: List[tuple] = []     # built cases waiting for the next round
+        group = None
+        running = False
+        hs: Dict[int, np.ndarray] = {}
+        pool = cf.ThreadPoolExecutor(max_workers=self.builders)
+        t0 = self.clock()
+        try:
+            while pending or queue or active or building or ready:
+                now = self.clock() - t0
+                while pending and pending[0].arrival_s <= now:
+                    queue.append(pending.popleft())
+                while queue and len(building) < self.builders and \
+                        len(active) + len(building) + len(ready) < self.max_active:
+                    req = queue[0]
+                    fp = self.footprint(req)
+                    if fp > self.hbm_budget:
+                        queue.popleft()
+                        results.append(Result(req.rid, req.npoints, req.nblocks, "rejected", 0, 0, req.arrival_s,
+                                              now, now, math.nan, math.nan))
+                        continue
+                    if used + fp > self.hbm_budget:
+                        break
+                    queue.popleft()
+                    used += fp
+                    building.append((pool.submit(self.make_case, req), req, fp))
+                while building and building[0][0].done():  # in admission order
+                    fut, req, fp = building.pop(0)
+                    ready.append((fut.result(), req, fp))
+                if running:
+                    for rid, slot in active.items():  # the group's stream: all finish together
+                        if rid not in hs:
+                            h = slot.fs.poll()
+                            if h is None:
+                                break
+                            hs[rid] = h
+                    if len(hs) < len(active):
+                        time.sleep(2e-4)
+                        continue
+                    running = False
+                    retired = []
+                    for rid, h in hs.items():
+                        slot = active[rid]
+                        slot.hist.append(h)
+                        slot.steps += len(h)
+                        res = self._retire_check(slot, self.clock() - t0)
+                        if res is not None:
+                            retired.append((rid, res))
+                    if retired or ready:
+                        if group is not None:
+                            group.close()
+                            group = None
+                        for rid, res in retired:
+                            slot = active.pop(rid)
+                            if self.keep_state:
+                                res.state = [slot.fs.download(b, "prim")[:5, 3:-3, 3:-3, 3:-3].copy()
+                                             for b in range(len(slot.fs.case.blocks))]
+                            slot.fs.close()
+                            used -= slot.footprint
+                            results.append(res)
+                if not running:
+                    if ready:
+                        if group is not None:
+                            group.close()
+                            group = None
+                        for fs, req, fp in ready:
+                            active[req.rid] = _Slot(req, fs, fp, self.clock() - t0)
+                        ready = []
+                        self.peak_resident = max(self.peak_resident, len(active))
+                        self.peak_bytes = max(self.peak_bytes, used)
+                    if active:
+                        if group is None:
+                            group = self.make_group([slot.fs for slot in active.values()])
+                        group.submit(self.quantum)
+                        running = True
+                        hs = {}  # this round's histories, per member
+                    else:
+                        time.sleep(2e-4)
+        finally:
+            pool.shutdown(wait=True)
+            if group is not None:
+                group.close()
+            for slot in active.values():
+                slot.fs.close()
+            for fs, _req, _fp in ready:
+                fs.close()
+        return sorted(results, key=lambda r: r.rid)
+
+    def _run_streams(self, requests: List[Request]) -> List[Result]:
         pending = deque(sorted(requests, key=lambda r: r.arrival_s))
         queue: deque = deque()
         active: Dict[int, _Slot] = {}

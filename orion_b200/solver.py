@@ -258,6 +258,50 @@ class FlowFieldSet:
         return conservative_from_prim(prim, self.params.gamma)
 
 
+class CaseGroup:
+    """Several device-resident cases stepped together: every stage is one
+    launch over the blocks of all members (orion_group_*).  Each member's
+    results are the same as when it steps alone; poll the members
+    (FlowFieldSet.poll) after submit().  Close the group before closing or
+    regrouping its members."""
+
+    def __init__(self, members: Sequence[FlowFieldSet]):
+        lib = _lib.load()
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m.handle for m in self.members])
+        h = C.c_void_p()
+        check(lib.orion_group_create(len(self.members), arr, C.byref(h)))
+        self._h = h
+
+    def submit(self, nsteps: int):
+        check(_lib.load().orion_group_submit(self._h, nsteps))
+
+    def sync(self):
+        check(_lib.load().orion_group_sync(self._h))
+
+    def step_launches(self) -> int:
+        v = C.c_int()
+        check(_lib.load().orion_group_step_launches(self._h, C.byref(v)))
+        return int(v.value)
+
+    def step(self, nsteps: int) -> List[np.ndarray]:
+        """Runs nsteps steps of every member; returns each member's history."""
+        self.submit(nsteps)
+        self.sync()
+        return [m.poll(max(nsteps, 1)) for m in self.members]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().orion_group_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def conservative_from_prim(prim: np.ndarray, gamma: float) -> np.ndarray:
     rho, u, v, w, p = prim[0], prim[1], prim[2], prim[3], prim[4]
     rc = np.where(rho < 0.0, np.abs(rho), rho)

@@ -5,7 +5,7 @@ small seeded cases.
     make -C oracle ref && python tests/golden/gen_golden.py [fixture ...]
 
 With no arguments it regenerates the small fixtures; the configuration
-horizons (c0_200, c1_40: minutes of reference CPU time) are made only when
+horizons (c0_200, c1_25: minutes of reference CPU time) are made only when
 named.
 
 Each fixture holds the case recipe, the reference's residual history
@@ -63,7 +63,7 @@ def interior_prim(state, sub: int = 1) -> np.ndarray:
 
 # The benchmark configurations at their own horizons (cases.config):
 #   c0_200: config 0 (one block 97x49x33) for its 200 steps;
-#   c1_40:  config 1 (eight blocks 193x97x65, split 2x2x2) for 40 steps, and the
+#   c1_25:  config 1 (eight blocks 193x97x65, split 2x2x2) for 25 steps, and the
 #           reference's residual history over its 300 steps (hist_long), which
 #           records where the reference's own scheme leaves convergence on this
 #           split.
@@ -71,7 +71,7 @@ def interior_prim(state, sub: int = 1) -> np.ndarray:
 # of the whole interior state beside it.
 HORIZONS = {
     "c0_200": dict(config=0, nsteps=200, sub=37, long_steps=0),
-    "c1_40": dict(config=1, nsteps=40, sub=211, long_steps=300),
+    "c1_25": dict(config=1, nsteps=25, sub=211, long_steps=300),
 }
 
 
@@ -99,10 +99,35 @@ def horizon(key: str, spec: dict) -> None:
     print(key, case.npoints, "points", case.nsteps, "steps", hist[-1, :2])
 
 
+# Two requests of the seeded serving stream (serving.c4_requests(24, seed=4))
+# whose flows diverge: the reference's residual history over 200 steps.
+DIVERGING = {"c4_diverging": dict(requests=24, seed=4, rids=(1, 18), steps=200)}
+
+
+def diverging(key: str, spec: dict) -> None:
+    from orion_b200 import serving
+
+    reqs = serving.c4_requests(spec["requests"], seed=spec["seed"], mean_ms=50.0, max_steps=spec["steps"])
+    hists = []
+    for rid in spec["rids"]:
+        case = reqs[rid].build_case()
+        case.nsteps = spec["steps"]
+        tmp = tempfile.mkdtemp(prefix="golden_")
+        cdir = os.path.join(tmp, "case")
+        case.write_reference_inputs(cdir)
+        refio.run_reference(cdir, spec["steps"], os.path.join(tmp, "out"), time_only=True)
+        hists.append(refio.read_hist(os.path.join(tmp, "out", "hist.bin")))
+        print(key, rid, case.npoints, "points", hists[-1][[0, -1], 0])
+    np.savez_compressed(os.path.join(HERE, key + ".npz"), hist=np.stack(hists), recipe=np.array([json.dumps(spec)]))
+
+
 def main(keys=None):
     for key, spec in HORIZONS.items():
         if keys and key in keys:
             horizon(key, spec)
+    for key, spec in DIVERGING.items():
+        if keys and key in keys:
+            diverging(key, spec)
     for key, recipe in RECIPES.items():
         if keys and key not in keys:
             continue

@@ -1,8 +1,9 @@
 """The request loop on the GPU: a request's result is the same alone and in a mix.
 
 Four small requests of different sizes and flow conditions are served once
-each on their own and once together (all resident at the same time, their
-steps overlapping on the device).  Tolerance: identical status and step
+each on their own and once together (all resident at the same time): in one
+group stepped with one launch per stage over all their blocks, or each on
+its own stream with their steps overlapping on the device.  Tolerance: identical status and step
 counts, and the final interior primitive state equal to 1e-12 relative (the
 kernels are deterministic, so in practice bit for bit).
 """
@@ -21,13 +22,14 @@ def _requests():
                             noise_seed=100 + i, max_steps=60, drop=1e-2) for i, (d, nb, m, re) in enumerate(spec)]
 
 
-def test_results_are_the_same_alone_and_in_the_mix():
+@pytest.mark.parametrize("batched", [True, False], ids=["group", "streams"])
+def test_results_are_the_same_alone_and_in_the_mix(batched):
     reqs = _requests()
     alone = {}
     for r in reqs:
-        srv = serving.Server(_lib.PREC_MIXED, quantum=10, keep_state=True)
+        srv = serving.Server(_lib.PREC_MIXED, quantum=10, keep_state=True, batched=False)
         alone[r.rid] = srv.run([r])[0]
-    srv = serving.Server(_lib.PREC_MIXED, quantum=10, keep_state=True)
+    srv = serving.Server(_lib.PREC_MIXED, quantum=10, keep_state=True, batched=batched)
     mixed = {r.rid: r for r in srv.run(reqs)}
     assert srv.peak_resident >= 2  # the requests really were resident together
     for rid, a in alone.items():
