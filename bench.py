@@ -9,7 +9,8 @@ seeded uneven blocks, Mach 0.8, Re 1e5, synthetic initial state (freestream +
 `value` is the mixed-precision batched path (FP32 flux / viscous / LU-SGS
 increments, FP64 metrics, Q update and norms); the plain FP64 path is timed
 beside it, and the relative L2 error of the mixed state against the plain
-state is taken after L2_STEPS steps from the same initial state.  Every GPU runs its own replica (weak scaling, no
+state is taken after L2_STEPS steps from the same initial state, and at
+several horizons of the workload and of configuration 0 (L2_HORIZONS).  Every GPU runs its own replica (weak scaling, no
 collective on the data path); times are CUDA events, max over ranks.
 
 --impl reference times the reference's own CPU implementation (compiled from
@@ -185,7 +186,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=24,
                     help="requests of the bounded serving run (0: skip it)")
-    ap.add_argument("--serve-max-steps", type=int, default=200)
+    ap.add_argument("--serve-max-steps", type=int, default=300)
+    ap.add_argument("--serve-drop", type=float, default=0.1,
+                    help="residual drop at which a served request retires (the bounded stream)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -233,10 +236,23 @@ def main():
     clocks = Clocks(local)
     results = {}
     states = {}
+    def interior(fs):
+        return [fs.download(b, "prim")[:5, 3:-3, 3:-3, 3:-3] for b in range(len(fs.case.blocks))]
+
+    def rel_l2(a, b):
+        num = sum(float(np.sum((x - y) ** 2)) for x, y in zip(a, b))
+        return (num / sum(float(np.sum(y ** 2)) for y in b)) ** 0.5
+
+    horizon_states = {}
     for name, prec in (("mixed", _lib.PREC_MIXED), ("plain", _lib.PREC_FP64)):
         fs = solver.FlowFieldSet(case, precision=prec, device=local)
-        fs.step(L2_STEPS)
-        states[name] = [fs.download(b, "prim")[:5, 3:-3, 3:-3, 3:-3] for b in range(len(case.blocks))]
+        done = 0
+        for hz in L2_HORIZONS["workload"]:
+            fs.step(hz - done)
+            done = hz
+            horizon_states[(name, "workload", hz)] = interior(fs)
+            if hz == L2_STEPS:
+                states[name] = horizon_states[(name, "workload", hz)]
         tune = fs.autotune(steps_per_trial=3)  # schedule chosen by timing on this case; solution unchanged
         fs.step(W)
         if name == "mixed":
@@ -246,10 +262,24 @@ def main():
                          "tune": tune}
         if name == "plain":
             clk = clocks.stop()
-    # L2 error of the mixed state against the plain FP64 state after L2_STEPS steps
-    num = sum(float(np.sum((m - p) ** 2)) for m, p in zip(states["mixed"], states["plain"]))
-    den = sum(float(np.sum(p ** 2)) for p in states["plain"])
-    l2 = (num / den) ** 0.5
+    # L2 error of the mixed state against the plain FP64 state after L2_STEPS
+    # steps, and at the horizons of the workload and of configuration 0
+    l2 = rel_l2(states["mixed"], states["plain"])
+    l2_horizons = {"workload": {str(hz): rel_l2(horizon_states[("mixed", "workload", hz)],
+                                                horizon_states[("plain", "workload", hz)])
+                                for hz in L2_HORIZONS["workload"]}}
+    c0 = cases.config(0)
+    c0_states = {}
+    for name, prec in (("mixed", _lib.PREC_MIXED), ("plain", _lib.PREC_FP64)):
+        f0 = solver.FlowFieldSet(c0, precision=prec, device=local)
+        done = 0
+        for hz in L2_HORIZONS["c0_97x49x33"]:
+            f0.step(hz - done)
+            done = hz
+            c0_states[(name, hz)] = interior(f0)
+        f0.close()
+    l2_horizons["c0_97x49x33"] = {str(hz): rel_l2(c0_states[("mixed", hz)], c0_states[("plain", hz)])
+                                  for hz in L2_HORIZONS["c0_97x49x33"]}
     per_rank_pts = npts * K
     mixed_ms, plain_ms = results["mixed"]["ms"], results["plain"]["ms"]
     value = group.aggregate_rate(per_rank_pts, mixed_ms / 1e3)
@@ -331,16 +361,28 @@ def main():
         from orion_b200 import serving
         for r in results.values():
             r["fs"].close()
-        reqs = serving.c4_requests(args.serve_requests, seed=4, mean_ms=50.0, max_steps=args.serve_max_steps)
-        srv = serving.Server(_lib.PREC_MIXED, device=local, quantum=20)
+        reqs = serving.c4_requests(args.serve_requests, seed=4, mean_ms=50.0, max_steps=args.serve_max_steps,
+                                   drop=args.serve_drop)
+        srv = serving.Server(_lib.PREC_MIXED, device=local, quantum=20)  # every resident case in one group
         mixed_s = serving.summarize(srv.run(reqs))
         mixed_s["peak_resident_cases"] = srv.peak_resident
-        seq = serving.Server(_lib.PREC_FP64, device=local, quantum=20, max_active=1)
+        mixed_s["mode"] = "group: one launch per stage over all resident cases"
+        srv_streams = serving.Server(_lib.PREC_MIXED, device=local, quantum=20, batched=False)
+        streams_s = serving.summarize(srv_streams.run(reqs))
+        streams_s["peak_resident_cases"] = srv_streams.peak_resident
+        streams_s["mode"] = "streams: every resident case on its own stream"
+        seq = serving.Server(_lib.PREC_FP64, device=local, quantum=20, max_active=1, batched=False)
         plain_s = serving.summarize(seq.run(reqs))
-        serving_out = {"requests": args.serve_requests, "max_steps": args.serve_max_steps, "drop": 1e-6,
+        peak, _kind = hbm_peak()
+        for sm, nb in ((mixed_s, STEP_BYTES[1]), (streams_s, STEP_BYTES[1]), (plain_s, STEP_BYTES[0])):
+            sm["hbm_gbs"] = sm["cell_updates_per_s"] * nb / 1e9
+            sm["hbm_frac"] = sm["hbm_gbs"] / peak
+        serving_out = {"requests": args.serve_requests, "max_steps": args.serve_max_steps, "drop": args.serve_drop,
                        "mean_interarrival_ms": 50.0,
-                       "mixed_continuous": mixed_s, "plain_one_at_a_time": plain_s,
-                       "throughput_ratio": mixed_s["cell_updates_per_s"] / plain_s["cell_updates_per_s"]}
+                       "mixed_continuous": mixed_s, "mixed_continuous_streams": streams_s,
+                       "plain_one_at_a_time": plain_s,
+                       "throughput_ratio": mixed_s["cell_updates_per_s"] / plain_s["cell_updates_per_s"],
+                       "vs_single_case_mixed": mixed_s["cell_updates_per_s"] / (value / world)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -363,6 +405,7 @@ def main():
             "sweep_schedule": {"mixed": results["mixed"]["sweeps"], "plain": results["plain"]["sweeps"]},
             "autotune": {"mixed": results["mixed"]["tune"], "plain": results["plain"]["tune"]},
             "mixed_vs_plain_rel_l2": l2, "mixed_vs_plain_l2_after_steps": L2_STEPS,
+            "mixed_vs_plain_rel_l2_horizons": l2_horizons,
             "roofline": roofline, "step_roofline": step_roofline,
             "stage_ms": stage_ms,
             "cpu_baseline": cpu,

@@ -158,6 +158,7 @@ struct orion_case_s {
   long long pending_first = 0;
   int pending_n = 0;
   struct orion_group_s* group = nullptr;  // the group the case steps in, if any
+  orion::ParamsDev* d_params = nullptr;   // device copy of P, read by the kernels through the blocks
 };
 
 // A group of cases stepped together: one launch per stage over all of their

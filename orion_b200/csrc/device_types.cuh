@@ -59,8 +59,8 @@ struct BlockDev {
   S* sk_pair;             // 30: per face neighbour q (lower i,j,k, upper i,j,k): l1, x1, x2, ct_n, rv/2
   S* sk_gm;               // 3 (static): |grad xi|, |grad eta|, |grad zeta| of the point's metrics
   S* sk_inv;              // 3 (static): 1 / max(|grad .|, 1e-30)
-  // the block's case parameters when it is stepped in a group of cases
-  // (orion_group_*); nullptr in a case's own descriptors, whose launches pass them
+  // the parameters of the block's case (a device copy): kernels read them
+  // here, so one launch can cover the blocks of several cases (orion_group_*)
   const ParamsDev* params;
 };
 

@@ -28,13 +28,6 @@ template <> struct FluxSrc<float> {
 };
 
 
-// The parameters of a block's case: its own copy when the block belongs to a
-// group of cases stepped together, else the launch's.
-template <typename S>
-__device__ __forceinline__ const ParamsDev& block_params(const BlockDev<S>& B, const ParamsDev& launch) {
-  return B.params ? *B.params : launch;
-}
-
 template <typename S>
 __device__ __forceinline__ long long lin(const BlockDev<S>& B, int i, int j, int k) {
   return (long long)i + (long long)B.nx * ((long long)j + (long long)B.ny * (long long)k);
@@ -116,12 +109,12 @@ __device__ __forceinline__ void dif_average(const BlockDev<S>& B, long long idx0
 
 template <typename S>
 __global__ void k_bc_phase(const BlockDev<S>* __restrict__ blocks, const RegionDev* __restrict__ regions,
-                           const int* __restrict__ phase_regions, ParamsDev P_launch) {
+                           const int* __restrict__ phase_regions) {
   const RegionDev R = regions[phase_regions[blockIdx.y]];
   const int pt = blockIdx.x * blockDim.x + threadIdx.x;
   if (pt >= R.npts) return;
   const BlockDev<S> B = blocks[R.block];
-  const ParamsDev& P = block_params(B, P_launch);
+  const ParamsDev& P = *B.params;
   const int wi = R.hi[0] - R.lo[0] + 1, wj = R.hi[1] - R.lo[1] + 1;
   const int i = R.lo[0] + pt % wi;
   const int j = R.lo[1] + (pt / wi) % wj;
@@ -456,11 +449,11 @@ __device__ __forceinline__ void dtmin_final_body(const double* __restrict__ part
 }
 
 template <typename S, bool DO_Q, bool DO_DT>
-__global__ void k_state(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P_launch,
+__global__ void k_state(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks,
                         double* __restrict__ dt_part) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const ParamsDev& P = block_params(B, P_launch);
+  const ParamsDev& P = *B.params;
   double local_min = 1000.0;
 #pragma unroll 4
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
@@ -487,11 +480,11 @@ __global__ void k_state(const BlockDev<S>* __restrict__ blocks, const Chunk* __r
 
 // time step alone (per-stage entry point): interior points of interior chunks
 template <typename S>
-__global__ void k_timestep(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P_launch,
-                           double* __restrict__ dt_part) {
+__global__ void k_timestep(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks,
+                        double* __restrict__ dt_part) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const ParamsDev& P = block_params(B, P_launch);
+  const ParamsDev& P = *B.params;
   double local_min = 1000.0;
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
     const long long n = ch.start + t;  // interior index
@@ -692,12 +685,12 @@ template <> struct LineMinBlocks<float> { static constexpr int visc = ORION_VISC
 template <> struct LineMinBlocks<double> { static constexpr int visc = ORION_VISC_MINB_F64, inv = ORION_INV_MINB_F64; };
 
 template <int D, typename S, typename T>
-__global__ void __launch_bounds__(256, LineMinBlocks<T>::visc) k_viscous(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles, ParamsDev P_launch) {
+__global__ void __launch_bounds__(256, LineMinBlocks<T>::visc) k_viscous(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* fsh = reinterpret_cast<T*>(smem_raw);
   const LineTile tl = tiles[blockIdx.x];
   const BlockDev<S> B = blocks[tl.block];
-  const ParamsDev& P = block_params(B, P_launch);
+  const ParamsDev& P = *B.params;
   const int L = dim_along(B, D);
   const int nf = L + 1;
   const long long st = stride_along(B, D);
@@ -969,12 +962,12 @@ __device__ void cascade_right(const BlockDev<S>& B, const InvLine<S, T>& ln, int
 }
 
 template <int D, typename S, typename T>
-__global__ void __launch_bounds__(256, LineMinBlocks<T>::inv) k_inviscid(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles, ParamsDev P_launch) {
+__global__ void __launch_bounds__(256, LineMinBlocks<T>::inv) k_inviscid(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* fsh = reinterpret_cast<T*>(smem_raw);
   const LineTile tl = tiles[blockIdx.x];
   const BlockDev<S> B = blocks[tl.block];
-  const ParamsDev& P = block_params(B, P_launch);
+  const ParamsDev& P = *B.params;
   const int L = dim_along(B, D);
   const int nf = L + 1;
   const long long st = stride_along(B, D);
@@ -1144,10 +1137,10 @@ __global__ void k_skew_static(const BlockDev<S>* __restrict__ blocks, int b) {
 // diagonal coefficient 1/(1/dt + sum of radii) (get_diag_coeff :267-295), the
 // same in all four sweeps.
 template <typename S, typename T, bool PAIRS = true>
-__global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P_launch) {
+__global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const ParamsDev& P = block_params(B, P_launch);
+  const ParamsDev& P = *B.params;
   const long long np = B.npad, nc = B.ncomp;
   const T gamma = T(P.gamma), reynolds = T(P.reynolds);
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
@@ -1217,10 +1210,10 @@ __global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk
 // x1, x2), ct_n, and half the viscous radius.  q = 0..2 lower i,j,k (sign +1),
 // q = 3..5 upper (sign -1).
 template <typename S, typename T>
-__global__ void k_sweep_pairs(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks, ParamsDev P_launch) {
+__global__ void k_sweep_pairs(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const ParamsDev& P = block_params(B, P_launch);
+  const ParamsDev& P = *B.params;
   const long long nc = B.ncomp;
   const T gamma = T(P.gamma);
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
@@ -1431,14 +1424,14 @@ __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefe
 #endif
 template <typename S, typename T, int MODE, int NT>
 __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
-                                                    const Chunk* __restrict__ chunks, ParamsDev P_launch) {
+                                                    const Chunk* __restrict__ chunks) {
   constexpr int Q0 = MODE == SW_LUSGS_BWD ? 3 : 0;
   constexpr int Q1 = MODE == SW_LUSGS_FWD ? 3 : 6;
   constexpr bool PRELOAD = sizeof(T) == 4;  // FP32: every static operand in registers before the wait
   const Chunk ch = chunks[blockIdx.x];
   const bool active = (int)threadIdx.x < ch.count;
   const BlockDev<S>& B = blocks[ch.block];
-  const ParamsDev& P = block_params(B, P_launch);
+  const ParamsDev& P = *B.params;
   const long long nc = B.ncomp;
   const int c = (int)ch.start + threadIdx.x;
   // pointers into registers now: griddepcontrol.wait clobbers memory, so
@@ -1757,14 +1750,13 @@ __device__ __forceinline__ void block_reduce_res(double& sum, double& mx, long l
 
 template <typename S, bool DO_RES, int NT>
 __global__ void __launch_bounds__(NT) k_sweep_finish(const BlockDev<S>* __restrict__ blocks,
-                                                     const Chunk* __restrict__ chunks, ParamsDev P_launch,
-                                                     ResPartial* __restrict__ partials) {
+                                                     const Chunk* __restrict__ chunks, ResPartial* __restrict__ partials) {
   // Natural order (interior index n = i + ni*(j + nj*k)): prim, dq, vol, dt
   // and the mask are read and written coalesced; only the swept increment is
   // gathered from the plane-major layout, at c = koff[s*nk + k] + (j - jlo(s,k)).
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const ParamsDev& P = block_params(B, P_launch);
+  const ParamsDev& P = *B.params;
   const long long np = B.npad, nc = B.ncomp;
   double sum = 0.0, mx = -1.0;
   long long key = (long long)0x7fffffffffffffffLL;
@@ -1896,10 +1888,10 @@ __device__ __forceinline__ void block_reduce_res(double& sum, double& mx, long l
 
 template <typename S, bool DO_UPDATE, bool DO_RES, int NT>
 __global__ void __launch_bounds__(NT) k_update_res(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks,
-                                                   ParamsDev P_launch, ResPartial* __restrict__ partials) {
+                                                    ResPartial* __restrict__ partials) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const ParamsDev& P = block_params(B, P_launch);
+  const ParamsDev& P = *B.params;
   const long long np = B.npad;
   double sum = 0.0, mx = -1.0;
   long long key = (long long)0x7fffffffffffffffLL;
@@ -2027,10 +2019,10 @@ __device__ __forceinline__ double splitmix_uniform(unsigned long long seed, unsi
 
 template <typename S>
 __global__ void k_init_flow(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks,
-                            const long long* __restrict__ pad_base, ParamsDev P_launch, unsigned long long seed, double amp) {
+                            const long long* __restrict__ pad_base, unsigned long long seed, double amp) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const ParamsDev& P = block_params(B, P_launch);
+  const ParamsDev& P = *B.params;
   const long long np = B.npad;
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
     const long long idx = ch.start + t;

@@ -127,7 +127,7 @@ void carve_block(char* base, const HostBlock& b, BlockDev<S>& d) {
   d.sk_pair = sk + 44 * nc;
   d.sk_gm = sk + 74 * nc;
   d.sk_inv = sk + 77 * nc;
-  d.params = nullptr;  // a case's own launches pass its parameters
+  d.params = nullptr;  // set by the caller: the case's device copy of its parameters
   d.ni = b.idim;
   d.nj = b.jdim;
   d.nk = b.kdim;
@@ -777,10 +777,15 @@ static int create_case(int nglobal, const orion_block_desc_t* blocks, const int*
   c->arena_bytes = total;
   CUDA_TRY(cudaMemsetAsync(c->arena, 0, total, c->stream));
   std::vector<long long> prim_off(nblocks);
+  // the case's parameters in device memory: every kernel reads them through
+  // its block's descriptor (so blocks of several cases can share a launch)
+  if ((rc = dev_alloc(c.get(), &c->d_params, 1))) return rc;
+  CUDA_TRY(cudaMemcpyAsync(c->d_params, &c->P, sizeof(ParamsDev), cudaMemcpyHostToDevice, c->stream));
   if (precision == ORION_PREC_FP64) {
     c->bd64.resize(nblocks);
     for (int b = 0; b < nblocks; ++b) {
       carve_block(static_cast<char*>(c->arena) + boff[b], c->hb[b], c->bd64[b]);
+      c->bd64[b].params = c->d_params;
       c->bd64[b].int_base = gint[plan.local[b]];
       prim_off[b] = (c->bd64[b].prim - static_cast<double*>(c->arena));
     }
@@ -791,6 +796,7 @@ static int create_case(int nglobal, const orion_block_desc_t* blocks, const int*
     c->bd32.resize(nblocks);
     for (int b = 0; b < nblocks; ++b) {
       carve_block(static_cast<char*>(c->arena) + boff[b], c->hb[b], c->bd32[b]);
+      c->bd32[b].params = c->d_params;
       c->bd32[b].int_base = gint[plan.local[b]];
       prim_off[b] = (c->bd32[b].prim - static_cast<double*>(c->arena));
     }
@@ -900,6 +906,9 @@ int orion_case_set_params(orion_case_t c, const orion_params_t* params) {
   if (!c || !params) return fail(ORION_E_INVALID, "null argument");
   std::lock_guard<std::mutex> lk(g_struct_mu);
   set_params_dev(c->P, *params);
+  // the device copy the kernels read, after the launches already enqueued
+  CUDA_TRY(cudaMemcpyAsync(c->d_params, &c->P, sizeof(ParamsDev), cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
   if (c->graph) {  // the captured step holds the old values: capture again on the next step
     cudaGraphExecDestroy(c->graph);
     c->graph = nullptr;
@@ -1441,17 +1450,11 @@ int build_group(orion_group_t g, orion_case_t px) {
   auto& mem = g->members;
   const int nm = (int)mem.size();
   int rc;
-  // block descriptors: the members' own, each pointing at its case's parameters
+  // block descriptors: the members' own
   std::vector<BlockDev<S>> blocks;
   std::vector<int> boff(nm + 1, 0);
-  ParamsDev* d_params = nullptr;
-  if ((rc = dev_alloc(px, &d_params, (size_t)nm))) return rc;
   for (int m = 0; m < nm; ++m) {
-    CUDA_TRY(cudaMemcpyAsync(d_params + m, &mem[m]->P, sizeof(ParamsDev), cudaMemcpyHostToDevice, px->stream));
-    for (auto b : host_blocks<S>(mem[m])) {
-      b.params = d_params + m;
-      blocks.push_back(b);
-    }
+    for (const auto& b : host_blocks<S>(mem[m])) blocks.push_back(b);  // each points at its case's parameters
     boff[m + 1] = (int)blocks.size();
   }
   BlockDev<S>* d_blocks = nullptr;

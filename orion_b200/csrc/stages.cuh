@@ -49,10 +49,10 @@ struct Stages {
   static int exchange(orion_case_t c) {
     auto& L = c->L;
     if (L.group) {
-      const GroupRun& G = *L.group;
-      if (G.n_halo > 0)
-        k_halo_copy_abs<<<(G.n_halo + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(G.halo_src, G.halo_dst,
-                                                                                          G.n_halo);
+      const GroupRun& GR = *L.group;
+      if (GR.n_halo > 0)
+        k_halo_copy_abs<<<(GR.n_halo + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(GR.halo_src, GR.halo_dst,
+                                                                                           GR.n_halo);
       return 0;
     }
     if (L.n_halo > 0)
@@ -67,7 +67,7 @@ struct Stages {
       const int nr = L.phase_off[p + 1] - L.phase_off[p];
       if (nr <= 0 || L.phase_maxpts[p] <= 0) continue;
       dim3 grid((L.phase_maxpts[p] + kThreads - 1) / kThreads, nr);
-      k_bc_phase<S><<<grid, kThreads, 0, c->stream>>>(blocks(c), L.regions, L.phase_regions + L.phase_off[p], c->P);
+      k_bc_phase<S><<<grid, kThreads, 0, c->stream>>>(blocks(c), L.regions, L.phase_regions + L.phase_off[p]);
     }
     return 0;
   }
@@ -75,13 +75,13 @@ struct Stages {
   static int state(orion_case_t c, bool with_dt, bool with_q) {
     auto& L = c->L;
     if (with_dt && with_q)
-      k_state<S, true, true><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dt_part);
+      k_state<S, true, true><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, L.dt_part);
     else if (with_dt)
-      k_state<S, false, true><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dt_part);
+      k_state<S, false, true><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, L.dt_part);
     else if (with_q)
-      k_state<S, true, false><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dt_part);
+      k_state<S, true, false><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, L.dt_part);
     else
-      k_state<S, false, false><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, c->P, L.dt_part);
+      k_state<S, false, false><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, L.dt_part);
     if (with_dt) {
       if (L.group)
         k_dtmin_group<<<L.group->nmembers, 1024, 0, c->stream>>>(L.group->members, L.dt_part);
@@ -93,7 +93,7 @@ struct Stages {
 
   static int timestep(orion_case_t c) {
     auto& L = c->L;
-    k_timestep<S><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P, L.dt_part);
+    k_timestep<S><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, L.dt_part);
     k_dtmin_final<<<1, 1024, 0, c->stream>>>(L.dt_part, L.n_int_chunks, L.dtmin);
     return 0;
   }
@@ -102,7 +102,7 @@ struct Stages {
   static void visc_dir(orion_case_t c) {
     auto& L = c->L;
     const size_t smem = (size_t)L.line_units[D] * 4 * sizeof(T);
-    k_viscous<D, S, T><<<L.n_tiles[D], kThreads, smem, c->stream>>>(blocks(c), L.tiles[D], c->P);
+    k_viscous<D, S, T><<<L.n_tiles[D], kThreads, smem, c->stream>>>(blocks(c), L.tiles[D]);
   }
 
   static int viscous(orion_case_t c) {
@@ -119,7 +119,7 @@ struct Stages {
   static void inv_dir(orion_case_t c) {
     auto& L = c->L;
     const size_t smem = (size_t)L.line_units[D] * 5 * sizeof(T);
-    k_inviscid<D, S, T><<<L.n_tiles[D], kThreads, smem, c->stream>>>(blocks(c), L.tiles[D], c->P);
+    k_inviscid<D, S, T><<<L.n_tiles[D], kThreads, smem, c->stream>>>(blocks(c), L.tiles[D]);
   }
 
   static int inviscid(orion_case_t c) {
@@ -170,7 +170,7 @@ struct Stages {
       cfg.attrs = attr;
       cfg.numAttrs = 1;
       CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweep_plane<S, T, MODE, NT>, blocks(c),
-                                  (const Chunk*)(L.sweep_chunks[dir] + off[t]), c->P));
+                                  (const Chunk*)(L.sweep_chunks[dir] + off[t])));
     }
     return 0;
   }
@@ -355,17 +355,17 @@ struct Stages {
     if (smem > kTileSmemMax) return fail(ORION_E_UNSUPPORTED, "block too long for the tile sweeps' row-base cache");
     k_sweep_tiles<S, T, MODE, DIR><<<n, 32 * TileShape<T>::TK + 32, smem, c->stream>>>(
         blocks(c), static_cast<const SweepTile*>(L.sweep_tiles[d]), n, static_cast<TileCtl*>(L.tile_ctl),
-        &sc->error, c->P, L.spin_limit);
+        &sc->error, L.spin_limit);
     return 0;
   }
 
   static int update(orion_case_t c, bool fuse_residual) {
     auto& L = c->L;
     if (L.tiles_on) {
-      k_lusgs_prep<S, T, false><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
+      k_lusgs_prep<S, T, false><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks);
     } else {
-      k_lusgs_prep<S, T, true><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
-      k_sweep_pairs<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P);
+      k_lusgs_prep<S, T, true><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks);
+      k_sweep_pairs<S, T><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks);
     }
     if (L.tiles_on) {
       int rc = tile_pass<SW_LUSGS_FWD, 1>(c);
@@ -387,11 +387,11 @@ struct Stages {
       if (rc) return rc;
     }
     if (fuse_residual) {
-      k_sweep_finish<S, true, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
+      k_sweep_finish<S, true, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks,
                                                                                      L.partials);
       residual_final(c);
     } else {
-      k_sweep_finish<S, false, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
+      k_sweep_finish<S, false, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks,
                                                                                       L.partials);
     }
     return 0;
@@ -422,7 +422,7 @@ struct Stages {
 
   static int residual(orion_case_t c) {
     auto& L = c->L;
-    k_update_res<S, false, true, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks, c->P,
+    k_update_res<S, false, true, kThreads><<<L.n_int_chunks, kThreads, 0, c->stream>>>(blocks(c), L.int_chunks,
                                                                                         L.partials);
     residual_final(c);
     return 0;
@@ -443,7 +443,7 @@ struct Stages {
 
   static int init_flow(orion_case_t c, uint64_t seed, double amp) {
     auto& L = c->L;
-    k_init_flow<S><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, L.pad_base, c->P, seed, amp);
+    k_init_flow<S><<<L.n_pad_chunks, kThreads, 0, c->stream>>>(blocks(c), L.pad_chunks, L.pad_base, seed, amp);
     return 0;
   }
 };

@@ -182,8 +182,7 @@ template <typename S, typename T, int MODE, int DIR>
 __global__ void __launch_bounds__(32 * TileShape<T>::TK + 32) k_sweep_tiles(const BlockDev<S>* __restrict__ blocks,
                                                                            const SweepTile* __restrict__ tiles,
                                                                            int ntiles, TileCtl* __restrict__ ctl,
-                                                                           int* __restrict__ err, ParamsDev P_launch,
-                                                                           long long spin_limit) {
+                                                                           int* __restrict__ err, long long spin_limit) {
   static_assert(sizeof(S) == sizeof(T), "the tile sweeps keep operands in their storage precision");
   constexpr int TJ = 32, TK = TileShape<T>::TK, PD = TileShape<T>::PD;
   constexpr int NSS = PD + 1, NSR = PD + 2, NR = tile_ring_fields<MODE>(), NS = kTileStatics;
@@ -206,7 +205,7 @@ __global__ void __launch_bounds__(32 * TileShape<T>::TK + 32) k_sweep_tiles(cons
   if (slot >= ntiles) return;
   const SweepTile W = tiles[slot];
   const BlockDev<S>& Bd = blocks[W.block];
-  const ParamsDev& P = block_params(Bd, P_launch);
+  const ParamsDev& P = *Bd.params;
   const int ni = Bd.ni;
   const int nsteps = ni + TJ + TK - 2;
 
