@@ -62,7 +62,7 @@ UPDATE_DRAM_BYTES_PER_POINT_MIXED = 1734.2e6 / 1254792
 # flow the reference's own scheme does not converge) and on configuration 0
 # (one block, converging).
 L2_STEPS = 10
-L2_HORIZONS = {"workload": (10, 30, 50), "c0_97x49x33": (10, 50, 100, 200)}
+L2_HORIZONS = {"workload": (10, 30, 50), "c0_97x49x33": (10, 50, 100, 200), "c2_289x161x65_27blk": (10, 50, 100)}
 # the reference-CPU leg of the line: timed steps after warm-up steps per process
 CPU_STEPS, CPU_WARMUP = 5, 2
 
@@ -268,18 +268,19 @@ def main():
     l2_horizons = {"workload": {str(hz): rel_l2(horizon_states[("mixed", "workload", hz)],
                                                 horizon_states[("plain", "workload", hz)])
                                 for hz in L2_HORIZONS["workload"]}}
-    c0 = cases.config(0)
-    c0_states = {}
-    for name, prec in (("mixed", _lib.PREC_MIXED), ("plain", _lib.PREC_FP64)):
-        f0 = solver.FlowFieldSet(c0, precision=prec, device=local)
-        done = 0
-        for hz in L2_HORIZONS["c0_97x49x33"]:
-            f0.step(hz - done)
-            done = hz
-            c0_states[(name, hz)] = interior(f0)
-        f0.close()
-    l2_horizons["c0_97x49x33"] = {str(hz): rel_l2(c0_states[("mixed", hz)], c0_states[("plain", hz)])
-                                  for hz in L2_HORIZONS["c0_97x49x33"]}
+    for cfg, key in ((0, "c0_97x49x33"), (2, "c2_289x161x65_27blk")):
+        cc = cases.config(cfg)
+        cc_states = {}
+        for name, prec in (("mixed", _lib.PREC_MIXED), ("plain", _lib.PREC_FP64)):
+            f0 = solver.FlowFieldSet(cc, precision=prec, device=local)
+            done = 0
+            for hz in L2_HORIZONS[key]:
+                f0.step(hz - done)
+                done = hz
+                cc_states[(name, hz)] = interior(f0)
+            f0.close()
+        l2_horizons[key] = {str(hz): rel_l2(cc_states[("mixed", hz)], cc_states[("plain", hz)])
+                            for hz in L2_HORIZONS[key]}
     per_rank_pts = npts * K
     mixed_ms, plain_ms = results["mixed"]["ms"], results["plain"]["ms"]
     value = group.aggregate_rate(per_rank_pts, mixed_ms / 1e3)

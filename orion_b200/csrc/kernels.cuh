@@ -1473,6 +1473,11 @@ __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane
       }
     }
   }
+  // the case's parameters loaded before the wait (after it they would be one
+  // more dependent load on the hyperplane chain) and used only after it: work
+  // before the wait that consumes its loads delays the chain
+  const double gamma_ld = P.gamma;
+  const int nvis = P.nvis;
   grid_dep_wait();
   grid_dep_launch();
   if (!active) return;
@@ -1486,7 +1491,7 @@ __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane
     if (nb[q] >= 0)
 #pragma unroll
       for (int m = 0; m < 5; ++m) dn[q][m] = (T)__ldcg(skdq + m * nc + nb[q]);
-  const T gm1 = T(P.gamma) - T(1);
+  const T gm1 = T(gamma_ld) - T(1);
   T rhs0[5] = {T(0), T(0), T(0), T(0), T(0)};
   // lower neighbours first (i, j, k), then upper (i, j, k): the reference's order
 #pragma unroll
@@ -1498,7 +1503,7 @@ __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane
       for (int k = 0; k < 5; ++k) pc[q][k] = (T)skpair[(5 * q + k) * nc + c];
       for (int k = 0; k < 3; ++k) nrm[d][k] = (T)sknrm[(3 * d + k) * nc + c];
     }
-    split_term<T, MODE>(q, gm1, P.nvis, dn[q], nq[q], pc[q], nrm[d], rhs0);
+    split_term<T, MODE>(q, gm1, nvis, dn[q], nq[q], pc[q], nrm[d], rhs0);
   }
 #pragma unroll
   for (int m = 0; m < 5; ++m) {

@@ -25,6 +25,8 @@ def main():
     ap.add_argument("--every", type=int, default=0, help="print every n-th step of the history (0: the last)")
     ap.add_argument("--time", action="store_true",
                     help="time the steps (CUDA events on the case's stream) and print cell-updates/s")
+    ap.add_argument("--autotune", action="store_true",
+                    help="autotune the schedule on the case first (the solution does not move) and print it")
     a = ap.parse_args()
     if a.small:
         case = cases.bump_case("profile_small", 97, 65, 49, split=(2, 2, 2), nsteps=a.steps)
@@ -33,6 +35,8 @@ def main():
     prec = _lib.PREC_MIXED if a.precision == "mixed" else _lib.PREC_FP64
     fs = solver.FlowFieldSet(case, precision=prec)
     fs.step(a.warmup)
+    if a.autotune:
+        print(json.dumps({"case": case.name, "precision": a.precision, "autotune": fs.autotune(steps_per_trial=3)}))
     if a.time:
         import torch
 
