@@ -239,6 +239,35 @@ int orion_case_autotune(orion_case_t c, int steps_per_trial, orion_schedule_t* t
 int orion_step_submit(orion_case_t c, int nsteps);
 int orion_case_poll(orion_case_t c, orion_residual_t* out, int cap, int* n);
 
+/* Pipelined host I/O of the primitive state ------------------------------
+ * The reference's driver loop reads and writes host arrays around every step
+ * (OrionSolver.cpp:139-209 over the host FlowFieldSet, FlowField.hpp:73-87);
+ * orion_case_upload / orion_case_download are that, one blocking copy at a
+ * time.  These calls stream states through a case with the copies overlapping
+ * the steps, for a sequence of independent inputs (each io step's input comes
+ * from the host, its result goes back to the host):
+ *   orion_io_put   enqueues the copy of one block's prim (6 x npad doubles,
+ *                  the upload layout) from PINNED host memory into the case's
+ *                  input staging, on the case's input copy stream;
+ *   orion_io_step  on the case's stream: installs the blocks put since the
+ *                  last io step into prim, runs nsteps whole steps with their
+ *                  residual history copied as orion_step_submit does (poll it
+ *                  with orion_case_poll), then copies prim to the output
+ *                  staging; returns at once;
+ *   orion_io_get   enqueues the copy of one block's prim as the last io step
+ *                  left it into PINNED host memory, on the output copy stream;
+ *   orion_io_wait  waits for every copy and step enqueued.
+ * The device orders them: a put issued after an io step starts once that step
+ * has installed the earlier puts, and an io step overwrites the output staging
+ * only after the gets of the previous one have read it.  Results are
+ * bit-identical to upload, step, download.  Host buffers stay untouched by the
+ * caller until orion_io_wait (pageable memory works but does not overlap).
+ * Not for shards or grouped cases. */
+int orion_io_put(orion_case_t c, int block, const double* host);
+int orion_io_step(orion_case_t c, int nsteps);
+int orion_io_get(orion_case_t c, int block, double* host);
+int orion_io_wait(orion_case_t c);
+
 /* Groups of cases: many cases, one launch per stage ------------------------
  * No single counterpart in the reference, which steps the blocks of one case
  * one after another in every stage (StateUpdater.cpp:544-580,

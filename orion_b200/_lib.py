@@ -71,6 +71,10 @@ SIGNATURES = {
                                       C.POINTER(Schedule)]),
     "orion_case_grid_metrics": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "orion_case_poll": (C.c_int, [C.c_void_p, C.POINTER(Residual), C.c_int, C.POINTER(C.c_int)]),
+    "orion_io_put": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "orion_io_step": (C.c_int, [C.c_void_p, C.c_int]),
+    "orion_io_get": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "orion_io_wait": (C.c_int, [C.c_void_p]),
     "orion_group_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "orion_group_submit": (C.c_int, [C.c_void_p, C.c_int]),
     "orion_group_sync": (C.c_int, [C.c_void_p]),

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "device_types.cuh"
@@ -49,9 +50,7 @@ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 struct GroupRun {
   GroupMember* members = nullptr;  // device array, one per case
   int nmembers = 0;
-  unsigned long long* halo_src = nullptr;  // halo copy as element addresses (the arenas differ)
-  unsigned long long* halo_dst = nullptr;
-  int n_halo = 0;
+  int max_halo = 0;                // the longest member halo copy list
 };
 
 struct DeviceLists {
@@ -132,6 +131,21 @@ struct ShardLists {
 
 }  // namespace orion
 
+// Pipelined host I/O (orion_io_*): staging copies of every block's prim and
+// the copy streams and events that order them against the steps.
+struct IoPipe {
+  cudaStream_t in = nullptr, out = nullptr;
+  double* stage_in = nullptr;
+  double* stage_out = nullptr;
+  std::vector<size_t> off;     // each block's prim in the staging buffers (doubles)
+  std::vector<uint8_t> put;    // blocks put since the last io step
+  cudaEvent_t in_ready = nullptr, in_free = nullptr, out_ready = nullptr, out_free = nullptr;
+  bool put_waits = false;      // the next put waits for in_free (an io step installed the staging)
+  bool step_waits = false;     // the next io step waits for out_free (gets read the staging)
+  bool get_waits = false;      // the next get waits for out_ready (a new io step filled the staging)
+  bool have_out = false;
+};
+
 struct orion_case_s {
   int nblocks = 0;
   int prec = ORION_PREC_FP64;
@@ -159,6 +173,10 @@ struct orion_case_s {
   int pending_n = 0;
   struct orion_group_s* group = nullptr;  // the group the case steps in, if any
   orion::ParamsDev* d_params = nullptr;   // device copy of P, read by the kernels through the blocks
+  // host copies of the work lists uploaded at set-up, by device address: a
+  // group is built from them without reading the lists back
+  std::unordered_map<const void*, std::vector<unsigned char>> list_mirror;
+  IoPipe* io = nullptr;  // orion_io_*, made on first use
 };
 
 // A group of cases stepped together: one launch per stage over all of their
@@ -169,6 +187,7 @@ struct orion_group_s {
   std::vector<cudaStream_t> saved_streams;  // the members' own streams, given back on destroy
   orion_case_s* proxy = nullptr;
   orion::GroupRun run;
+  std::vector<int> block_off;  // each member's first block in the group's descriptors
 };
 
 namespace orion {

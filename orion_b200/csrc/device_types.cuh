@@ -62,6 +62,11 @@ struct BlockDev {
   // the parameters of the block's case (a device copy): kernels read them
   // here, so one launch can cover the blocks of several cases (orion_group_*)
   const ParamsDev* params;
+  // the two parameters the hyperplane sweeps read, copied here so that they
+  // arrive with the block's own fields (one dependent load fewer on the sweep
+  // chain); equal to params->gamma and params->nvis
+  double sweep_gamma;
+  int sweep_nvis;
 };
 
 // Scalar parameters (orion_params_t after conversion).
@@ -135,6 +140,11 @@ struct GroupMember {
   ResidualOut* hist;             // the case's history ring
   int* counter;
   ResPartial* total;
+  // the case's own halo copy list (element indices into its arena)
+  double* arena;
+  const long long* halo_src;
+  const long long* halo_dst;
+  int n_halo;
 };
 
 }  // namespace orion

@@ -69,11 +69,13 @@ static __global__ void k_halo_copy(double* __restrict__ arena, const long long* 
   if (t < n) arena[dst[t]] = arena[src[t]];
 }
 
-// The same copy for a group of cases, whose arenas differ: element addresses.
-static __global__ void k_halo_copy_abs(const unsigned long long* __restrict__ src,
-                                       const unsigned long long* __restrict__ dst, int n) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) *reinterpret_cast<double*>(dst[t]) = *reinterpret_cast<const double*>(src[t]);
+// The same copy for a group of cases: blockIdx.y is the member, which copies
+// through its own list into its own arena (nothing is concatenated).
+static __global__ void k_halo_copy_group(const GroupMember* __restrict__ members) {
+  const GroupMember& M = members[blockIdx.y];
+  double* const arena = M.arena;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < M.n_halo; t += gridDim.x * blockDim.x)
+    arena[M.halo_dst[t]] = arena[M.halo_src[t]];
 }
 
 // ===========================================================================
@@ -1343,8 +1345,8 @@ __device__ __forceinline__ void sweep_fetch(const BlockDev<S>& B, int block, int
 // operands (dn: neighbour increment; nq: u, v, w, H, c2, af of the neighbour;
 // pc: l1, x1, x2, ct_n, rv/2 of the pair; nrm: the point's unit normal).
 template <typename T, int MODE>
-__device__ __forceinline__ void split_term(int q, T gm1, int nvis, const T dn[5], const T nq[6], const T pc[5],
-                                           const T nrm[3], T rhs0[5]) {
+__device__ __forceinline__ void split_flux(int q, T gm1, int nvis, const T dn[5], const T nq[6], const T pc[5],
+                                           const T nrm[3], T fs[5]) {
   const T drm = dn[0], dum = dn[1], dvm = dn[2], dwm = dn[3], dEm = dn[4];
   const T um = nq[0], vm = nq[1], wm = nq[2], H = nq[3], c2 = nq[4], af = nq[5];
   const T nx_n = nrm[0], ny_n = nrm[1], nz_n = nrm[2];
@@ -1352,7 +1354,6 @@ __device__ __forceinline__ void split_term(int q, T gm1, int nvis, const T dn[5]
   const T dc = ct_n * drm - (nx_n * dum + ny_n * dvm + nz_n * dwm);
   const T dh = af * drm - gm1 * (um * dum + vm * dvm + wm * dwm - dEm);
   const T c2dc = c2 * dc;
-  T fs[5];
   fs[0] = l1 * drm - dh * x1 - dc * x2;
   fs[1] = l1 * dum + (nx_n * c2dc - um * dh) * x1 + (nx_n * dh - um * dc) * x2;
   fs[2] = l1 * dvm + (ny_n * c2dc - vm * dh) * x1 + (ny_n * dh - vm * dc) * x2;
@@ -1366,11 +1367,23 @@ __device__ __forceinline__ void split_term(int q, T gm1, int nvis, const T dn[5]
       for (int m = 0; m < 5; ++m) fs[m] += rvh * dn[m];
     }
   }
+}
+
+template <typename T, int MODE>
+__device__ __forceinline__ void split_accumulate(int q, const T fs[5], T rhs0[5]) {
   if (MODE == SW_GS && q >= 3) {
     for (int m = 0; m < 5; ++m) rhs0[m] -= fs[m];
   } else {
     for (int m = 0; m < 5; ++m) rhs0[m] += fs[m];
   }
+}
+
+template <typename T, int MODE>
+__device__ __forceinline__ void split_term(int q, T gm1, int nvis, const T dn[5], const T nq[6], const T pc[5],
+                                           const T nrm[3], T rhs0[5]) {
+  T fs[5];
+  split_flux<T, MODE>(q, gm1, nvis, dn, nq, pc, nrm, fs);
+  split_accumulate<T, MODE>(q, fs, rhs0);
 }
 
 template <typename S, typename T, int MODE>
@@ -1422,16 +1435,30 @@ __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefe
 #ifndef ORION_SWEEP_SM_THREADS
 #define ORION_SWEEP_SM_THREADS 512
 #endif
-template <typename S, typename T, int MODE, int NT>
+// DIR: +1 for a pass over increasing hyperplanes, -1 for decreasing.  In a GS
+// pass one side's neighbours are not written during the pass (the upper ones
+// going forward, the lower ones going backward: they hold the previous pass's
+// increments, complete before this pass began), so their terms are formed
+// before the wait; after it only the other side's are.  The terms are still
+// summed in the reference's order (lower i, j, k, then upper i, j, k).
+template <typename S, typename T, int MODE, int NT, int DIR>
 __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
                                                     const Chunk* __restrict__ chunks) {
   constexpr int Q0 = MODE == SW_LUSGS_BWD ? 3 : 0;
   constexpr int Q1 = MODE == SW_LUSGS_FWD ? 3 : 6;
+  constexpr bool GS = MODE == SW_GS;
+  constexpr int E0 = GS ? (DIR > 0 ? 3 : 0) : 0;  // neighbours formed before the wait: [E0, E1)
+  constexpr int E1 = GS ? (DIR > 0 ? 6 : 3) : 0;
+  constexpr int F0 = GS ? (DIR > 0 ? 0 : 3) : Q0;  // neighbours written just before: [F0, F1)
+  constexpr int F1 = GS ? (DIR > 0 ? 3 : 6) : Q1;
   constexpr bool PRELOAD = sizeof(T) == 4;  // FP32: every static operand in registers before the wait
   const Chunk ch = chunks[blockIdx.x];
   const bool active = (int)threadIdx.x < ch.count;
   const BlockDev<S>& B = blocks[ch.block];
-  const ParamsDev& P = *B.params;
+  // the case's parameters, from the block's own descriptor (loaded with its
+  // other fields; a further dependent load would lengthen the chain)
+  const double gamma_ld = B.sweep_gamma;
+  const int nvis = B.sweep_nvis;
   const long long nc = B.ncomp;
   const int c = (int)ch.start + threadIdx.x;
   // pointers into registers now: griddepcontrol.wait clobbers memory, so
@@ -1443,6 +1470,7 @@ __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane
   int nb[6];
   T coed = T(0), own[5];
   T nq[6][6], pc[6][5], nrm[3][3];
+  T early[3][5];  // GS: the terms of neighbours [E0, E1)
   if (active) {
 #pragma unroll
     for (int q = Q0; q < Q1; ++q) nb[q] = B.sk_nb[q * nc + c];
@@ -1451,7 +1479,7 @@ __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane
 #pragma unroll
       for (int m = 0; m < 5; ++m) own[m] = -(T)B.sk_rhs[m * nc + c];
 #pragma unroll
-    for (int q = Q0; q < Q1; ++q) {
+    for (int q = F0; q < F1; ++q) {
       if (nb[q] < 0) continue;
       if (PRELOAD) {
 #pragma unroll
@@ -1465,29 +1493,39 @@ __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      if (PRELOAD) {
+      if (PRELOAD || GS) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) nrm[d][k] = (T)B.sk_nrm[(3 * d + k) * nc + c];
       } else {
         for (int k = 0; k < 3; ++k) prefetch_l2(B.sk_nrm + (long long)(3 * d + k) * nc + c);
       }
     }
+    if (GS) {
+      const T gm1e = T(gamma_ld) - T(1);
+#pragma unroll
+      for (int q = E0; q < E1; ++q) {
+        if (nb[q] < 0) continue;
+        T dn[5], nqe[6], pce[5];
+#pragma unroll
+        for (int m = 0; m < 5; ++m) dn[m] = (T)__ldcg(B.sk_dq + m * nc + nb[q]);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) nqe[k] = (T)B.sk_nbq[k * nc + nb[q]];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) pce[k] = (T)B.sk_pair[(5 * q + k) * nc + c];
+        split_flux<T, MODE>(q, gm1e, nvis, dn, nqe, pce, nrm[q % 3], early[q - E0]);
+      }
+    }
   }
-  // the case's parameters loaded before the wait (after it they would be one
-  // more dependent load on the hyperplane chain) and used only after it: work
-  // before the wait that consumes its loads delays the chain
-  const double gamma_ld = P.gamma;
-  const int nvis = P.nvis;
   grid_dep_wait();
   grid_dep_launch();
   if (!active) return;
   if (MODE == SW_LUSGS_BWD)  // the forward increment: the launch just before may have written it
 #pragma unroll
     for (int m = 0; m < 5; ++m) own[m] = (T)__ldcg(skdq + m * nc + c);
-  // every neighbour increment in flight at once
+  // every fresh neighbour increment in flight at once
   T dn[6][5];
 #pragma unroll
-  for (int q = Q0; q < Q1; ++q)
+  for (int q = F0; q < F1; ++q)
     if (nb[q] >= 0)
 #pragma unroll
       for (int m = 0; m < 5; ++m) dn[q][m] = (T)__ldcg(skdq + m * nc + nb[q]);
@@ -1497,11 +1535,16 @@ __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane
 #pragma unroll
   for (int q = Q0; q < Q1; ++q) {
     if (nb[q] < 0) continue;
+    if (q >= E0 && q < E1) {
+      split_accumulate<T, MODE>(q, early[q - E0], rhs0);
+      continue;
+    }
     const int d = q % 3;
     if (!PRELOAD) {
       for (int k = 0; k < 6; ++k) nq[q][k] = (T)sknbq[k * nc + nb[q]];
       for (int k = 0; k < 5; ++k) pc[q][k] = (T)skpair[(5 * q + k) * nc + c];
-      for (int k = 0; k < 3; ++k) nrm[d][k] = (T)sknrm[(3 * d + k) * nc + c];
+      if (!GS)
+        for (int k = 0; k < 3; ++k) nrm[d][k] = (T)sknrm[(3 * d + k) * nc + c];
     }
     split_term<T, MODE>(q, gm1, nvis, dn[q], nq[q], pc[q], nrm[d], rhs0);
   }

@@ -28,7 +28,7 @@ int set_error(int code, const std::string& msg) { return fail(code, msg); }
 namespace {
 
 template <typename T>
-int dev_upload(orion_case_t c, T** dptr, const std::vector<T>& v) {
+int dev_upload(orion_case_t c, T** dptr, const std::vector<T>& v, bool keep = false) {
   *dptr = nullptr;
   if (v.empty()) return 0;
   void* p = nullptr;
@@ -36,6 +36,10 @@ int dev_upload(orion_case_t c, T** dptr, const std::vector<T>& v) {
     return fail(ORION_E_NOMEM, "cudaMallocAsync (work list)");
   c->allocs.push_back(p);
   CUDA_TRY(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+  if (keep) {  // a list a group is built from
+    const auto* bytes = reinterpret_cast<const unsigned char*>(v.data());
+    c->list_mirror[p].assign(bytes, bytes + v.size() * sizeof(T));
+  }
   *dptr = static_cast<T*>(p);
   return 0;
 }
@@ -286,7 +290,7 @@ int build_line_tiles(orion_case_t c) {
       const int nlines = d == 0 ? h.jdim * h.kdim : (d == 1 ? h.idim * h.kdim : h.idim * h.jdim);
       for (int s = 0; s < nlines; s += lanes) tiles.push_back(LineTile{b, s, std::min(lanes, nlines - s), 0});
     }
-    if ((rc = dev_upload(c, &L.tiles[d], tiles))) return rc;
+    if ((rc = dev_upload(c, &L.tiles[d], tiles, true))) return rc;
     L.n_tiles[d] = (int)tiles.size();
   }
   return 0;
@@ -349,7 +353,7 @@ int build_sweep_tiles(orion_case_t c) {
     }
     int rc;
     SweepTile* d = nullptr;
-    if ((rc = dev_upload(c, &d, tiles))) return rc;
+    if ((rc = dev_upload(c, &d, tiles, true))) return rc;
     L.sweep_tiles[dir] = d;
     L.n_sweep_tiles[dir] = (int)tiles.size();
     maxn = std::max(maxn, (int)tiles.size());
@@ -374,9 +378,9 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off, const Ex
     for (long long s = 0; s < ni; s += kChunk) itr.push_back(Chunk{b, (int)std::min<long long>(kChunk, ni - s), s});
   }
   int rc;
-  if ((rc = dev_upload(c, &L.pad_chunks, pad))) return rc;
+  if ((rc = dev_upload(c, &L.pad_chunks, pad, true))) return rc;
   L.n_pad_chunks = (int)pad.size();
-  if ((rc = dev_upload(c, &L.int_chunks, itr))) return rc;
+  if ((rc = dev_upload(c, &L.int_chunks, itr, true))) return rc;
   L.n_int_chunks = (int)itr.size();
   if ((rc = dev_upload(c, &L.pad_base, c->shard.pad_base))) return rc;
 
@@ -422,7 +426,7 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off, const Ex
         }
         off.push_back((int)ch.size());
       }
-      if ((rc = dev_upload(c, &L.sweep_chunks[dir], ch))) return rc;
+      if ((rc = dev_upload(c, &L.sweep_chunks[dir], ch, true))) return rc;
       if ((rc = dev_upload(c, &L.sweep_off_dev[dir], off))) return rc;
       L.sweep_off[dir] = off;
     }
@@ -502,21 +506,21 @@ int build_lists(orion_case_t c, const std::vector<long long>& prim_off, const Ex
       L.phase_off.push_back((int)phase_list.size());
       L.phase_maxpts.push_back(maxpts);
     }
-    if ((rc = dev_upload(c, &L.regions, regs))) return rc;
-    if ((rc = dev_upload(c, &L.phase_regions, phase_list))) return rc;
+    if ((rc = dev_upload(c, &L.regions, regs, true))) return rc;
+    if ((rc = dev_upload(c, &L.phase_regions, phase_list, true))) return rc;
   }
 
   // ---------------- interface residual averaging ----------------
   // own slots are packed here; the slots of other shards arrive after them
   {
-    if ((rc = dev_upload(c, &L.pk_block, plan.pk_block))) return rc;
-    if ((rc = dev_upload(c, &L.pk_idx, plan.pk_idx))) return rc;
+    if ((rc = dev_upload(c, &L.pk_block, plan.pk_block, true))) return rc;
+    if ((rc = dev_upload(c, &L.pk_idx, plan.pk_idx, true))) return rc;
     L.n_pack = (int)plan.pk_block.size();
     if ((rc = dev_alloc(c, &L.pack, (size_t)plan.n_slots * 5))) return rc;
-    if ((rc = dev_upload(c, &L.ap_block, plan.ap_block))) return rc;
-    if ((rc = dev_upload(c, &L.ap_idx, plan.ap_idx))) return rc;
-    if ((rc = dev_upload(c, &L.ap_off, plan.ap_off))) return rc;
-    if ((rc = dev_upload(c, &L.ap_slot, plan.ap_slot))) return rc;
+    if ((rc = dev_upload(c, &L.ap_block, plan.ap_block, true))) return rc;
+    if ((rc = dev_upload(c, &L.ap_idx, plan.ap_idx, true))) return rc;
+    if ((rc = dev_upload(c, &L.ap_off, plan.ap_off, true))) return rc;
+    if ((rc = dev_upload(c, &L.ap_slot, plan.ap_slot, true))) return rc;
     L.n_ap = (int)plan.ap_block.size();
     auto& X = c->shard;
     X.iface_send.assign(plan.nranks, nullptr);
@@ -588,9 +592,12 @@ static void release_hist_ring(ResidualOut* r) {
   g_free_rings.push_back(r);
 }
 
+void io_release(orion_case_t c);
+
 void destroy_case(orion_case_t c) {
   if (!c) return;
   if (c->graph) cudaGraphExecDestroy(c->graph);
+  io_release(c);
   // stream-ordered frees: no device-wide synchronisation while other cases run
   for (void* p : c->allocs) cudaFreeAsync(p, c->stream);
   if (c->arena) cudaFreeAsync(c->arena, c->stream);
@@ -786,6 +793,8 @@ static int create_case(int nglobal, const orion_block_desc_t* blocks, const int*
     for (int b = 0; b < nblocks; ++b) {
       carve_block(static_cast<char*>(c->arena) + boff[b], c->hb[b], c->bd64[b]);
       c->bd64[b].params = c->d_params;
+      c->bd64[b].sweep_gamma = c->P.gamma;
+      c->bd64[b].sweep_nvis = c->P.nvis;
       c->bd64[b].int_base = gint[plan.local[b]];
       prim_off[b] = (c->bd64[b].prim - static_cast<double*>(c->arena));
     }
@@ -797,6 +806,8 @@ static int create_case(int nglobal, const orion_block_desc_t* blocks, const int*
     for (int b = 0; b < nblocks; ++b) {
       carve_block(static_cast<char*>(c->arena) + boff[b], c->hb[b], c->bd32[b]);
       c->bd32[b].params = c->d_params;
+      c->bd32[b].sweep_gamma = c->P.gamma;
+      c->bd32[b].sweep_nvis = c->P.nvis;
       c->bd32[b].int_base = gint[plan.local[b]];
       prim_off[b] = (c->bd32[b].prim - static_cast<double*>(c->arena));
     }
@@ -902,12 +913,44 @@ int orion_case_set_stream(orion_case_t c, void* stream) {
   return 0;
 }
 
+}  // extern "C"
+
+namespace {
+
+template <typename S>
+int refresh_blocks(orion_case_t c, std::vector<BlockDev<S>>& bd) {
+  for (auto& b : bd) {
+    b.sweep_gamma = c->P.gamma;
+    b.sweep_nvis = c->P.nvis;
+  }
+  if (bd.empty()) return 0;
+  CUDA_TRY(cudaMemcpyAsync(c->d_blocks, bd.data(), sizeof(BlockDev<S>) * bd.size(), cudaMemcpyHostToDevice, c->stream));
+  if (c->group) {
+    const auto& mem = c->group->members;
+    const size_t m = std::find(mem.begin(), mem.end(), c) - mem.begin();
+    auto* gb = static_cast<BlockDev<S>*>(c->group->proxy->d_blocks) + c->group->block_off[m];
+    CUDA_TRY(cudaMemcpyAsync(gb, bd.data(), sizeof(BlockDev<S>) * bd.size(), cudaMemcpyHostToDevice, c->stream));
+  }
+  return 0;
+}
+
+int refresh_block_params(orion_case_t c) {
+  return c->prec == ORION_PREC_FP64 ? refresh_blocks<double>(c, c->bd64) : refresh_blocks<float>(c, c->bd32);
+}
+
+}  // namespace
+
+extern "C" {
+
 int orion_case_set_params(orion_case_t c, const orion_params_t* params) {
   if (!c || !params) return fail(ORION_E_INVALID, "null argument");
   std::lock_guard<std::mutex> lk(g_struct_mu);
   set_params_dev(c->P, *params);
   // the device copy the kernels read, after the launches already enqueued
   CUDA_TRY(cudaMemcpyAsync(c->d_params, &c->P, sizeof(ParamsDev), cudaMemcpyHostToDevice, c->stream));
+  // and the sweeps' copies in the block descriptors (the case's, and its group's)
+  int rc = refresh_block_params(c);
+  if (rc) return rc;
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   if (c->graph) {  // the captured step holds the old values: capture again on the next step
     cudaGraphExecDestroy(c->graph);
@@ -1410,6 +1453,61 @@ int orion_case_poll(orion_case_t c, orion_residual_t* out, int cap, int* n) {
   return 1;
 }
 
+}  // extern "C"
+
+// ---- pipelined host I/O (orion_io_*) -------------------------------------
+namespace {
+
+int io_pipe(orion_case_t c, IoPipe** out) {
+  if (c->io) {
+    *out = c->io;
+    return 0;
+  }
+  if (c->group) return fail(ORION_E_UNSUPPORTED, "a grouped case steps through its group");
+  if (c->shard.nranks > 1) return fail(ORION_E_UNSUPPORTED, "a shard exchanges through its own calls");
+  auto io = std::make_unique<IoPipe>();
+  size_t total = 0;
+  for (int b = 0; b < c->nblocks; ++b) {
+    io->off.push_back(total);
+    total += (size_t)c->hb[b].npad * 6;
+  }
+  io->put.assign(c->nblocks, 0);
+  auto cleanup = [&](const char* what) {
+    if (io->stage_in) cudaFree(io->stage_in);
+    if (io->stage_out) cudaFree(io->stage_out);
+    return fail(ORION_E_NOMEM, what);
+  };
+  if (cudaMalloc((void**)&io->stage_in, total * sizeof(double)) != cudaSuccess) return cleanup("input staging");
+  if (cudaMalloc((void**)&io->stage_out, total * sizeof(double)) != cudaSuccess) return cleanup("output staging");
+  CUDA_TRY(cudaStreamCreateWithFlags(&io->in, cudaStreamNonBlocking));
+  CUDA_TRY(cudaStreamCreateWithFlags(&io->out, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&io->in_ready, &io->in_free, &io->out_ready, &io->out_free})
+    CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  c->io = io.release();
+  *out = c->io;
+  return 0;
+}
+
+void io_release(orion_case_t c) {
+  IoPipe* io = c->io;
+  if (!io) return;
+  if (io->in) cudaStreamSynchronize(io->in);
+  if (io->out) cudaStreamSynchronize(io->out);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(io->stage_in);
+  cudaFree(io->stage_out);
+  for (cudaEvent_t e : {io->in_ready, io->in_free, io->out_ready, io->out_free})
+    if (e) cudaEventDestroy(e);
+  if (io->in) cudaStreamDestroy(io->in);
+  if (io->out) cudaStreamDestroy(io->out);
+  delete io;
+  c->io = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
 int orion_last_residual(orion_case_t c, orion_residual_t* out) {
   if (!c || !out) return fail(ORION_E_INVALID, "null argument");
   int cnt = 0;
@@ -1417,6 +1515,95 @@ int orion_last_residual(orion_case_t c, orion_residual_t* out) {
   CUDA_TRY(cudaMemcpy(&cnt, c->L.counter, sizeof(int), cudaMemcpyDeviceToHost));
   if (cnt <= 0) return fail(ORION_E_INVALID, "no step has run");
   return read_hist(c, cnt - 1, 1, out);
+}
+
+
+int orion_io_put(orion_case_t c, int block, const double* host) {
+  if (!c || !host || block < 0 || block >= c->nblocks) return fail(ORION_E_INVALID, "bad arguments");
+  IoPipe* io = nullptr;
+  int rc = io_pipe(c, &io);
+  if (rc) return rc;
+  if (io->put_waits) {  // the last io step must have installed the staging first
+    CUDA_TRY(cudaStreamWaitEvent(io->in, io->in_free, 0));
+    io->put_waits = false;
+  }
+  CUDA_TRY(cudaMemcpyAsync(io->stage_in + io->off[block], host, sizeof(double) * 6 * (size_t)c->hb[block].npad,
+                           cudaMemcpyHostToDevice, io->in));
+  io->put[block] = 1;
+  return 0;
+}
+
+int orion_io_step(orion_case_t c, int nsteps) {
+  if (!c || nsteps < 0) return fail(ORION_E_INVALID, "bad arguments");
+  IoPipe* io = nullptr;
+  int rc = io_pipe(c, &io);
+  if (rc) return rc;
+  if (c->pending_n + nsteps > kHistCap)
+    return fail(ORION_E_INVALID, "more unpolled steps than the history ring holds (4096)");
+  // install the blocks put since the last io step
+  bool any = false;
+  for (int b = 0; b < c->nblocks; ++b) any = any || io->put[b];
+  if (any) {
+    CUDA_TRY(cudaEventRecord(io->in_ready, io->in));
+    CUDA_TRY(cudaStreamWaitEvent(c->stream, io->in_ready, 0));
+    for (int b = 0; b < c->nblocks; ++b) {
+      if (!io->put[b]) continue;
+      void* d;
+      int nc;
+      bool st;
+      if ((rc = field_info(c, b, ORION_FIELD_PRIM, &d, &nc, &st))) return rc;
+      CUDA_TRY(cudaMemcpyAsync(d, io->stage_in + io->off[b], sizeof(double) * 6 * (size_t)c->hb[b].npad,
+                               cudaMemcpyDeviceToDevice, c->stream));
+      rc = dispatch(c, [&](const StageOps& o) { return o.prim_shadow(c, b); });
+      if (rc) return rc;
+      io->put[b] = 0;
+    }
+    CUDA_TRY(cudaEventRecord(io->in_free, c->stream));
+    io->put_waits = true;
+  }
+  if ((rc = orion_step_submit(c, nsteps))) return rc;
+  // the result into the output staging, once the previous gets have read it
+  if (io->step_waits) {
+    CUDA_TRY(cudaEventRecord(io->out_free, io->out));
+    CUDA_TRY(cudaStreamWaitEvent(c->stream, io->out_free, 0));
+    io->step_waits = false;
+  }
+  for (int b = 0; b < c->nblocks; ++b) {
+    void* d;
+    int nc;
+    bool st;
+    if ((rc = field_info(c, b, ORION_FIELD_PRIM, &d, &nc, &st))) return rc;
+    CUDA_TRY(cudaMemcpyAsync(io->stage_out + io->off[b], d, sizeof(double) * 6 * (size_t)c->hb[b].npad,
+                             cudaMemcpyDeviceToDevice, c->stream));
+  }
+  CUDA_TRY(cudaEventRecord(io->out_ready, c->stream));
+  io->get_waits = true;
+  io->have_out = true;
+  return 0;
+}
+
+int orion_io_get(orion_case_t c, int block, double* host) {
+  if (!c || !host || block < 0 || block >= c->nblocks) return fail(ORION_E_INVALID, "bad arguments");
+  IoPipe* io = c->io;
+  if (!io || !io->have_out) return fail(ORION_E_INVALID, "no io step has run");
+  if (io->get_waits) {
+    CUDA_TRY(cudaStreamWaitEvent(io->out, io->out_ready, 0));
+    io->get_waits = false;
+  }
+  CUDA_TRY(cudaMemcpyAsync(host, io->stage_out + io->off[block], sizeof(double) * 6 * (size_t)c->hb[block].npad,
+                           cudaMemcpyDeviceToHost, io->out));
+  io->step_waits = true;
+  return 0;
+}
+
+int orion_io_wait(orion_case_t c) {
+  if (!c) return fail(ORION_E_INVALID, "null case");
+  if (c->io) {
+    CUDA_TRY(cudaStreamSynchronize(c->io->in));
+    CUDA_TRY(cudaStreamSynchronize(c->io->out));
+  }
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return sweep_status(c);
 }
 
 }  // extern "C"
@@ -1430,10 +1617,17 @@ int orion_last_residual(orion_case_t c, orion_residual_t* out) {
 // ---------------------------------------------------------------------------
 namespace {
 
+// A member's list: its set-up copy when it has one, else read back.
 template <typename T>
-int download(std::vector<T>& v, const T* d, size_t n) {
+int download(orion_case_t c, std::vector<T>& v, const T* d, size_t n) {
   v.resize(n);
-  if (n) CUDA_TRY(cudaMemcpy(v.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost));
+  if (!n) return 0;
+  auto it = c->list_mirror.find(static_cast<const void*>(d));
+  if (it != c->list_mirror.end() && it->second.size() >= n * sizeof(T)) {
+    std::memcpy(v.data(), it->second.data(), n * sizeof(T));
+    return 0;
+  }
+  CUDA_TRY(cudaMemcpy(v.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost));
   return 0;
 }
 
@@ -1467,7 +1661,6 @@ int build_group(orion_group_t g, orion_case_t px) {
   std::vector<GroupMember> gm(nm);
   std::vector<Chunk> pad, itr;
   std::vector<LineTile> tl[3];
-  std::vector<unsigned long long> hsrc, hdst;
   std::vector<RegionDev> regs;
   std::vector<std::vector<int>> phases;
   std::vector<int> pk_block, ap_block, ap_off{0}, ap_slot;
@@ -1481,11 +1674,11 @@ int build_group(orion_group_t g, orion_case_t px) {
     const int bo = boff[m];
     std::vector<Chunk> v;
     // padded and interior chunks; the member's partial ranges
-    if ((rc = download(v, M.pad_chunks, M.n_pad_chunks))) return rc;
+    if ((rc = download(c, v, M.pad_chunks, M.n_pad_chunks))) return rc;
     gm[m].pad_off = (int)pad.size();
     gm[m].pad_n = M.n_pad_chunks;
     for (auto ch : v) { ch.block += bo; pad.push_back(ch); }
-    if ((rc = download(v, M.int_chunks, M.n_int_chunks))) return rc;
+    if ((rc = download(c, v, M.int_chunks, M.n_int_chunks))) return rc;
     gm[m].part_off = (int)itr.size();
     gm[m].part_n = M.n_int_chunks;
     for (auto ch : v) { ch.block += bo; itr.push_back(ch); }
@@ -1499,31 +1692,27 @@ int build_group(orion_group_t g, orion_case_t px) {
     // line tiles
     for (int d = 0; d < 3; ++d) {
       std::vector<LineTile> t;
-      if ((rc = download(t, M.tiles[d], M.n_tiles[d]))) return rc;
+      if ((rc = download(c, t, M.tiles[d], M.n_tiles[d]))) return rc;
       for (auto x : t) { x.block += bo; tl[d].push_back(x); }
       L.lanes[d] = std::max(L.lanes[d], M.lanes[d]);
       L.lmax[d] = std::max(L.lmax[d], M.lmax[d]);
       L.line_units[d] = std::max(L.line_units[d], M.line_units[d]);
     }
-    // halo copy as element addresses
-    {
-      std::vector<long long> a, b;
-      if ((rc = download(a, M.halo_src, M.n_halo)) || (rc = download(b, M.halo_dst, M.n_halo))) return rc;
-      const unsigned long long base = (unsigned long long)(uintptr_t)c->arena;
-      for (int q = 0; q < M.n_halo; ++q) {
-        hsrc.push_back(base + 8ull * (unsigned long long)a[q]);
-        hdst.push_back(base + 8ull * (unsigned long long)b[q]);
-      }
-    }
+    // halo copy: the member's own list, read in place
+    gm[m].arena = static_cast<double*>(c->arena);
+    gm[m].halo_src = M.halo_src;
+    gm[m].halo_dst = M.halo_dst;
+    gm[m].n_halo = M.n_halo;
+    g->run.max_halo = std::max(g->run.max_halo, M.n_halo);
     // physical BC phases: the p-th region of every block of every member
     {
       std::vector<RegionDev> r;
       std::vector<int> pl;
       const int nreg = M.phase_off.empty() ? 0 : M.phase_off.back();
-      if ((rc = download(pl, M.phase_regions, (size_t)nreg))) return rc;
+      if ((rc = download(c, pl, M.phase_regions, (size_t)nreg))) return rc;
       int maxr = 0;
       for (int x : pl) maxr = std::max(maxr, x + 1);
-      if ((rc = download(r, M.regions, (size_t)maxr))) return rc;
+      if ((rc = download(c, r, M.regions, (size_t)maxr))) return rc;
       const int rbase = (int)regs.size();
       for (auto x : r) { x.block += bo; regs.push_back(x); }
       for (size_t p = 0; p + 1 < M.phase_off.size(); ++p) {
@@ -1535,10 +1724,10 @@ int build_group(orion_group_t g, orion_case_t px) {
     {
       std::vector<int> pb, ab, ao, as;
       std::vector<long long> pi, ai;
-      if ((rc = download(pb, M.pk_block, M.n_pack)) || (rc = download(pi, M.pk_idx, M.n_pack))) return rc;
-      if ((rc = download(ab, M.ap_block, M.n_ap)) || (rc = download(ai, M.ap_idx, M.n_ap))) return rc;
-      if ((rc = download(ao, M.ap_off, M.n_ap ? (size_t)M.n_ap + 1 : 0))) return rc;
-      if ((rc = download(as, M.ap_slot, M.n_ap ? (size_t)ao.back() : 0))) return rc;
+      if ((rc = download(c, pb, M.pk_block, M.n_pack)) || (rc = download(c, pi, M.pk_idx, M.n_pack))) return rc;
+      if ((rc = download(c, ab, M.ap_block, M.n_ap)) || (rc = download(c, ai, M.ap_idx, M.n_ap))) return rc;
+      if ((rc = download(c, ao, M.ap_off, M.n_ap ? (size_t)M.n_ap + 1 : 0))) return rc;
+      if ((rc = download(c, as, M.ap_slot, M.n_ap ? (size_t)ao.back() : 0))) return rc;
       const int slot_base = (int)pk_block.size(), ent_base = (int)ap_slot.size();
       for (int q = 0; q < M.n_pack; ++q) { pk_block.push_back(pb[q] + bo); pk_idx.push_back(pi[q]); }
       for (int q = 0; q < M.n_ap; ++q) {
@@ -1556,7 +1745,7 @@ int build_group(orion_group_t g, orion_case_t px) {
       const auto& off = M.sweep_off[dir];
       if (!off.empty()) {
         std::vector<Chunk> ch;
-        if ((rc = download(ch, M.sweep_chunks[dir], (size_t)off.back()))) return rc;
+        if ((rc = download(c, ch, M.sweep_chunks[dir], (size_t)off.back()))) return rc;
         const int np = (int)off.size() - 1;
         if ((int)planes[dir].size() < np) planes[dir].resize(np);
         for (int t = 0; t < np; ++t)
@@ -1567,7 +1756,7 @@ int build_group(orion_group_t g, orion_case_t px) {
           }
       }
       std::vector<SweepTile> st;
-      if ((rc = download(st, static_cast<const SweepTile*>(M.sweep_tiles[dir]), (size_t)M.n_sweep_tiles[dir])))
+      if ((rc = download(c, st, static_cast<const SweepTile*>(M.sweep_tiles[dir]), (size_t)M.n_sweep_tiles[dir])))
         return rc;
       const int sb = (int)stiles[dir].size();
       for (auto x : st) {
@@ -1589,8 +1778,6 @@ int build_group(orion_group_t g, orion_case_t px) {
     L.n_tiles[d] = (int)tl[d].size();
   }
   GroupRun& G = g->run;
-  if ((rc = dev_upload(px, &G.halo_src, hsrc)) || (rc = dev_upload(px, &G.halo_dst, hdst))) return rc;
-  G.n_halo = (int)hsrc.size();
   {
     std::vector<int> plist;
     L.phase_off.assign(1, 0);
@@ -1643,6 +1830,7 @@ int build_group(orion_group_t g, orion_case_t px) {
   if ((rc = dev_alloc(px, &L.dt_part, (size_t)std::max(L.n_pad_chunks, 1)))) return rc;
   if ((rc = dev_upload(px, &G.members, gm))) return rc;
   G.nmembers = nm;
+  g->block_off.assign(boff.begin(), boff.end() - 1);
   L.group = &G;
   return 0;
 }

@@ -50,9 +50,11 @@ struct Stages {
     auto& L = c->L;
     if (L.group) {
       const GroupRun& GR = *L.group;
-      if (GR.n_halo > 0)
-        k_halo_copy_abs<<<(GR.n_halo + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(GR.halo_src, GR.halo_dst,
-                                                                                           GR.n_halo);
+      if (GR.max_halo > 0) {
+        // grid-stride per member: four CTAs per SM of a B200 (148 SMs) cover the longest list
+        const int gx = std::min((GR.max_halo + kThreads - 1) / kThreads, 4 * 148);
+        k_halo_copy_group<<<dim3(gx, GR.nmembers), kThreads, 0, c->stream>>>(GR.members);
+      }
       return 0;
     }
     if (L.n_halo > 0)
@@ -169,8 +171,16 @@ struct Stages {
       cfg.stream = c->stream;
       cfg.attrs = attr;
       cfg.numAttrs = 1;
-      CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweep_plane<S, T, MODE, NT>, blocks(c),
-                                  (const Chunk*)(L.sweep_chunks[dir] + off[t])));
+      const Chunk* ch = L.sweep_chunks[dir] + off[t];
+      if constexpr (MODE == SW_GS) {  // the pass direction decides which neighbours are formed early
+        if (dir == 0) {
+          CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweep_plane<S, T, MODE, NT, 1>, blocks(c), ch));
+        } else {
+          CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweep_plane<S, T, MODE, NT, -1>, blocks(c), ch));
+        }
+      } else {
+        CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweep_plane<S, T, MODE, NT, MODE == SW_LUSGS_FWD ? 1 : -1>, blocks(c), ch));
+      }
     }
     return 0;
   }

@@ -136,6 +136,12 @@ class FlowFieldSet:
     def sync(self):
         check(_lib.load().orion_case_sync(self._h))
 
+    def set_params(self, params: FlowParams):
+        """Replaces the flow parameters for the steps enqueued from now on
+        (orion_case_set_params); a grouped case keeps stepping in its group."""
+        check(_lib.load().orion_case_set_params(self._h, C.byref(_params_struct(params))))
+        self.params = params
+
     def stream_ptr(self) -> int:
         v = C.c_void_p()
         check(_lib.load().orion_case_stream(self._h, C.byref(v)))
@@ -245,6 +251,36 @@ class FlowFieldSet:
             out[s, 2:7] = list(r.max_loc)
             out[s, 7] = r.phydtime
         return out
+
+    # -- pipelined host I/O: copies overlap the steps (orion_io_*) --------
+    def _prim_buffer(self, block: int, arr) -> int:
+        nx, ny, nz = self.case.blocks[block].padded
+        n = 6 * nx * ny * nz
+        if isinstance(arr, np.ndarray):
+            if arr.dtype != np.float64 or not arr.flags.c_contiguous or arr.size != n:
+                raise OrionError(f"prim of block {block}: a C-contiguous float64 array of {n} values")
+            return arr.ctypes.data
+        if arr.dtype.itemsize != 8 or not arr.is_contiguous() or arr.numel() != n:  # a (pinned) torch tensor
+            raise OrionError(f"prim of block {block}: a contiguous float64 tensor of {n} values")
+        return arr.data_ptr()
+
+    def io_put(self, block: int, prim):
+        """Enqueues the copy of a block's prim from host memory (pinned: a
+        torch tensor from pin_memory(), for the copy to overlap the steps)."""
+        check(_lib.load().orion_io_put(self._h, block, self._prim_buffer(block, prim)))
+
+    def io_step(self, nsteps: int = 1):
+        """Installs the blocks put since the last io step, enqueues nsteps steps
+        (history as submit(); poll it) and the copy of the result to staging."""
+        check(_lib.load().orion_io_step(self._h, nsteps))
+
+    def io_get(self, block: int, prim):
+        """Enqueues the copy of a block's prim, as the last io step left it, into
+        host memory; valid after io_wait()."""
+        check(_lib.load().orion_io_get(self._h, block, self._prim_buffer(block, prim)))
+
+    def io_wait(self):
+        check(_lib.load().orion_io_wait(self._h))
 
     def last_residual(self) -> ResidualStats:
         r = _lib.Residual()

@@ -87,3 +87,35 @@ def test_submit_and_poll_continue_after_the_group():
     assert np.array_equal(np.vstack([h1, h2]), h_ref)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("precision", [_lib.PREC_FP64, _lib.PREC_MIXED], ids=["plain", "mixed"])
+def test_new_parameters_reach_a_grouped_member(precision):
+    """orion_case_set_params on a member of a group: its next steps use the new
+    gamma, viscosity switch and CFL (the block descriptors the group's sweeps
+    read are refreshed), exactly as when the case steps alone."""
+    import dataclasses
+
+    def changed(p):
+        return dataclasses.replace(p, gamma=1.3, cfl=0.5 * p.cfl)
+
+    ref = []
+    for sp in SPECS:
+        fs = solver.FlowFieldSet(cases.small_case(**sp), precision=precision)
+        h1 = fs.step(3)
+        if sp["name"] == "g1":
+            fs.set_params(changed(fs.params))
+        h2 = fs.step(3)
+        ref.append((np.concatenate([h1, h2]), _state(fs)))
+        fs.close()
+    members = [solver.FlowFieldSet(cases.small_case(**sp), precision=precision) for sp in SPECS]
+    g = solver.CaseGroup(members)
+    h1 = g.step(3)
+    members[1].set_params(changed(members[1].params))
+    h2 = g.step(3)
+    g.close()
+    for (h_a, st_a), a1, a2, fs in zip(ref, h1, h2, members):
+        assert np.array_equal(h_a, np.concatenate([a1, a2]))
+        for a, b in zip(st_a, _state(fs)):
+            assert np.array_equal(a, b)
+        fs.close()
