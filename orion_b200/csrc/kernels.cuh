@@ -1435,28 +1435,20 @@ __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefe
 #ifndef ORION_SWEEP_SM_THREADS
 #define ORION_SWEEP_SM_THREADS 512
 #endif
-// DIR: +1 for a pass over increasing hyperplanes, -1 for decreasing.  In a GS
-// pass one side's neighbours are not written during the pass (the upper ones
-// going forward, the lower ones going backward: they hold the previous pass's
-// increments, complete before this pass began), so their terms are formed
-// before the wait; after it only the other side's are.  The terms are still
-// summed in the reference's order (lower i, j, k, then upper i, j, k).
-template <typename S, typename T, int MODE, int NT, int DIR>
+template <typename S, typename T, int MODE, int NT>
 __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane(const BlockDev<S>* __restrict__ blocks,
                                                     const Chunk* __restrict__ chunks) {
   constexpr int Q0 = MODE == SW_LUSGS_BWD ? 3 : 0;
   constexpr int Q1 = MODE == SW_LUSGS_FWD ? 3 : 6;
-  constexpr bool GS = MODE == SW_GS;
-  constexpr int E0 = GS ? (DIR > 0 ? 3 : 0) : 0;  // neighbours formed before the wait: [E0, E1)
-  constexpr int E1 = GS ? (DIR > 0 ? 6 : 3) : 0;
-  constexpr int F0 = GS ? (DIR > 0 ? 0 : 3) : Q0;  // neighbours written just before: [F0, F1)
-  constexpr int F1 = GS ? (DIR > 0 ? 3 : 6) : Q1;
   constexpr bool PRELOAD = sizeof(T) == 4;  // FP32: every static operand in registers before the wait
   const Chunk ch = chunks[blockIdx.x];
   const bool active = (int)threadIdx.x < ch.count;
   const BlockDev<S>& B = blocks[ch.block];
-  // the case's parameters, from the block's own descriptor (loaded with its
-  // other fields; a further dependent load would lengthen the chain)
+  // the case's parameters, from the block's own descriptor: loaded with its
+  // other fields and used only after the wait.  Work before the wait beyond
+  // issuing loads lengthens the chain: it competes with the previous
+  // hyperplane's launch, which is still running on the same SMs (forming a GS
+  // pass's stale-side terms there, or even gamma - 1, made the step slower).
   const double gamma_ld = B.sweep_gamma;
   const int nvis = B.sweep_nvis;
   const long long nc = B.ncomp;
@@ -1470,7 +1462,6 @@ __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane
   int nb[6];
   T coed = T(0), own[5];
   T nq[6][6], pc[6][5], nrm[3][3];
-  T early[3][5];  // GS: the terms of neighbours [E0, E1)
   if (active) {
 #pragma unroll
     for (int q = Q0; q < Q1; ++q) nb[q] = B.sk_nb[q * nc + c];
@@ -1479,7 +1470,7 @@ __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane
 #pragma unroll
       for (int m = 0; m < 5; ++m) own[m] = -(T)B.sk_rhs[m * nc + c];
 #pragma unroll
-    for (int q = F0; q < F1; ++q) {
+    for (int q = Q0; q < Q1; ++q) {
       if (nb[q] < 0) continue;
       if (PRELOAD) {
 #pragma unroll
@@ -1493,26 +1484,11 @@ __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      if (PRELOAD || GS) {
+      if (PRELOAD) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) nrm[d][k] = (T)B.sk_nrm[(3 * d + k) * nc + c];
       } else {
         for (int k = 0; k < 3; ++k) prefetch_l2(B.sk_nrm + (long long)(3 * d + k) * nc + c);
-      }
-    }
-    if (GS) {
-      const T gm1e = T(gamma_ld) - T(1);
-#pragma unroll
-      for (int q = E0; q < E1; ++q) {
-        if (nb[q] < 0) continue;
-        T dn[5], nqe[6], pce[5];
-#pragma unroll
-        for (int m = 0; m < 5; ++m) dn[m] = (T)__ldcg(B.sk_dq + m * nc + nb[q]);
-#pragma unroll
-        for (int k = 0; k < 6; ++k) nqe[k] = (T)B.sk_nbq[k * nc + nb[q]];
-#pragma unroll
-        for (int k = 0; k < 5; ++k) pce[k] = (T)B.sk_pair[(5 * q + k) * nc + c];
-        split_flux<T, MODE>(q, gm1e, nvis, dn, nqe, pce, nrm[q % 3], early[q - E0]);
       }
     }
   }
@@ -1522,10 +1498,10 @@ __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane
   if (MODE == SW_LUSGS_BWD)  // the forward increment: the launch just before may have written it
 #pragma unroll
     for (int m = 0; m < 5; ++m) own[m] = (T)__ldcg(skdq + m * nc + c);
-  // every fresh neighbour increment in flight at once
+  // every neighbour increment in flight at once
   T dn[6][5];
 #pragma unroll
-  for (int q = F0; q < F1; ++q)
+  for (int q = Q0; q < Q1; ++q)
     if (nb[q] >= 0)
 #pragma unroll
       for (int m = 0; m < 5; ++m) dn[q][m] = (T)__ldcg(skdq + m * nc + nb[q]);
@@ -1535,16 +1511,11 @@ __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane
 #pragma unroll
   for (int q = Q0; q < Q1; ++q) {
     if (nb[q] < 0) continue;
-    if (q >= E0 && q < E1) {
-      split_accumulate<T, MODE>(q, early[q - E0], rhs0);
-      continue;
-    }
     const int d = q % 3;
     if (!PRELOAD) {
       for (int k = 0; k < 6; ++k) nq[q][k] = (T)sknbq[k * nc + nb[q]];
       for (int k = 0; k < 5; ++k) pc[q][k] = (T)skpair[(5 * q + k) * nc + c];
-      if (!GS)
-        for (int k = 0; k < 3; ++k) nrm[d][k] = (T)sknrm[(3 * d + k) * nc + c];
+      for (int k = 0; k < 3; ++k) nrm[d][k] = (T)sknrm[(3 * d + k) * nc + c];
     }
     split_term<T, MODE>(q, gm1, nvis, dn[q], nq[q], pc[q], nrm[d], rhs0);
   }

@@ -999,7 +999,7 @@ int orion_case_get_schedule(orion_case_t c, orion_schedule_t* s) {
 
 static int launch_steps(orion_case_t c, int nsteps);
 static int sweep_status(orion_case_t c);
-static int enqueue_hist_copy(orion_case_t c, int nsteps);
+static int enqueue_hist_copy(orion_case_t c, int nsteps, cudaStream_t st = nullptr);
 
 int orion_case_autotune(orion_case_t c, int steps_per_trial, orion_schedule_t* trials, int cap, int* ntrials,
                         orion_schedule_t* best) {
@@ -1409,7 +1409,8 @@ int orion_step_submit(orion_case_t c, int nsteps) {
 
 // Copies the history entries of the last nsteps steps (enqueued on the case's
 // stream) into the case's pinned ring and records them as pending.
-static int enqueue_hist_copy(orion_case_t c, int nsteps) {
+static int enqueue_hist_copy(orion_case_t c, int nsteps, cudaStream_t st) {
+  // on the case's stream unless another stream ordered after the steps is given;
   // the new entries sit at ring positions [first, first + nsteps) mod kHistCap
   const long long first = c->hist_count;
   long long pos = first % kHistCap;
@@ -1417,7 +1418,7 @@ static int enqueue_hist_copy(orion_case_t c, int nsteps) {
   while (left > 0) {
     const int n = (int)std::min<long long>(left, kHistCap - pos);
     CUDA_TRY(cudaMemcpyAsync(c->hist_host + pos, c->L.hist + pos, sizeof(ResidualOut) * n, cudaMemcpyDeviceToHost,
-                             c->stream));
+                             st ? st : c->stream));
     left -= n;
     pos = 0;
   }
@@ -1430,6 +1431,14 @@ static int enqueue_hist_copy(orion_case_t c, int nsteps) {
 int orion_case_poll(orion_case_t c, orion_residual_t* out, int cap, int* n) {
   if (!c || !n || (cap > 0 && !out)) return fail(ORION_E_INVALID, "null argument");
   *n = 0;
+  if (c->io) {  // pipelined I/O copies the history on the output copy stream
+    const cudaError_t qo = cudaStreamQuery(c->io->out);
+    if (qo == cudaErrorNotReady) return 0;
+    if (qo != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ORION_E_CUDA, std::string("output copy stream: ") + cudaGetErrorString(qo));
+    }
+  }
   const cudaError_t q = cudaStreamQuery(c->stream);
   if (q == cudaErrorNotReady) return 0;
   if (q != cudaSuccess) {
@@ -1458,6 +1467,29 @@ int orion_case_poll(orion_case_t c, orion_residual_t* out, int cap, int* n) {
 // ---- pipelined host I/O (orion_io_*) -------------------------------------
 namespace {
 
+// Staging copies on the SMs: a cudaMemcpyAsync between device buffers would
+// queue on the copy engines behind the host copies of the neighbouring steps.
+__global__ void k_copy_doubles(const double* __restrict__ src, double* __restrict__ dst, long long n) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0) {
+    const long long n2 = n / 2;
+    for (long long i = t; i < n2; i += stride)
+      reinterpret_cast<double2*>(dst)[i] = reinterpret_cast<const double2*>(src)[i];
+    if (t == 0 && (n & 1)) dst[n - 1] = src[n - 1];
+  } else {
+    for (long long i = t; i < n; i += stride) dst[i] = src[i];
+  }
+}
+
+int copy_doubles(const double* src, double* dst, long long n, cudaStream_t st) {
+  const long long want = (n / 2 + 255) / 256;
+  const int grid = (int)std::max<long long>(1, std::min<long long>(want, 148LL * 8));
+  k_copy_doubles<<<grid, 256, 0, st>>>(src, dst, n);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
 int io_pipe(orion_case_t c, IoPipe** out) {
   if (c->io) {
     *out = c->io;
@@ -1469,7 +1501,7 @@ int io_pipe(orion_case_t c, IoPipe** out) {
   size_t total = 0;
   for (int b = 0; b < c->nblocks; ++b) {
     io->off.push_back(total);
-    total += (size_t)c->hb[b].npad * 6;
+    total += ((size_t)c->hb[b].npad * 6 + 1) / 2 * 2;  // 16-byte aligned starts
   }
   io->put.assign(c->nblocks, 0);
   auto cleanup = [&](const char* what) {
@@ -1552,8 +1584,9 @@ int orion_io_step(orion_case_t c, int nsteps) {
       int nc;
       bool st;
       if ((rc = field_info(c, b, ORION_FIELD_PRIM, &d, &nc, &st))) return rc;
-      CUDA_TRY(cudaMemcpyAsync(d, io->stage_in + io->off[b], sizeof(double) * 6 * (size_t)c->hb[b].npad,
-                               cudaMemcpyDeviceToDevice, c->stream));
+      if ((rc = copy_doubles(io->stage_in + io->off[b], static_cast<double*>(d), 6 * (long long)c->hb[b].npad,
+                             c->stream)))
+        return rc;
       rc = dispatch(c, [&](const StageOps& o) { return o.prim_shadow(c, b); });
       if (rc) return rc;
       io->put[b] = 0;
@@ -1561,7 +1594,14 @@ int orion_io_step(orion_case_t c, int nsteps) {
     CUDA_TRY(cudaEventRecord(io->in_free, c->stream));
     io->put_waits = true;
   }
-  if ((rc = orion_step_submit(c, nsteps))) return rc;
+  if (!c->hist_host && !(c->hist_host = acquire_hist_ring())) return fail(ORION_E_NOMEM, "pinned history ring");
+  if (c->hist_count < 0) {  // once: learn the device counter
+    int cnt = 0;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    CUDA_TRY(cudaMemcpy(&cnt, c->L.counter, sizeof(int), cudaMemcpyDeviceToHost));
+    c->hist_count = cnt;
+  }
+  if (nsteps > 0 && (rc = launch_steps(c, nsteps))) return rc;
   // the result into the output staging, once the previous gets have read it
   if (io->step_waits) {
     CUDA_TRY(cudaEventRecord(io->out_free, io->out));
@@ -1573,11 +1613,17 @@ int orion_io_step(orion_case_t c, int nsteps) {
     int nc;
     bool st;
     if ((rc = field_info(c, b, ORION_FIELD_PRIM, &d, &nc, &st))) return rc;
-    CUDA_TRY(cudaMemcpyAsync(io->stage_out + io->off[b], d, sizeof(double) * 6 * (size_t)c->hb[b].npad,
-                             cudaMemcpyDeviceToDevice, c->stream));
+    if ((rc = copy_doubles(static_cast<const double*>(d), io->stage_out + io->off[b], 6 * (long long)c->hb[b].npad,
+                           c->stream)))
+      return rc;
   }
   CUDA_TRY(cudaEventRecord(io->out_ready, c->stream));
-  io->get_waits = true;
+  // the residual history leaves with the state, on the output copy stream: on
+  // the case's stream that small copy would queue on the copy engine behind
+  // the previous state's copy to the host and hold up the next step
+  CUDA_TRY(cudaStreamWaitEvent(io->out, io->out_ready, 0));
+  if (nsteps > 0 && (rc = enqueue_hist_copy(c, nsteps, io->out))) return rc;
+  io->get_waits = false;
   io->have_out = true;
   return 0;
 }

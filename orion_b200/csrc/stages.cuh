@@ -171,16 +171,8 @@ struct Stages {
       cfg.stream = c->stream;
       cfg.attrs = attr;
       cfg.numAttrs = 1;
-      const Chunk* ch = L.sweep_chunks[dir] + off[t];
-      if constexpr (MODE == SW_GS) {  // the pass direction decides which neighbours are formed early
-        if (dir == 0) {
-          CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweep_plane<S, T, MODE, NT, 1>, blocks(c), ch));
-        } else {
-          CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweep_plane<S, T, MODE, NT, -1>, blocks(c), ch));
-        }
-      } else {
-        CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweep_plane<S, T, MODE, NT, MODE == SW_LUSGS_FWD ? 1 : -1>, blocks(c), ch));
-      }
+      CUDA_TRY(cudaLaunchKernelEx(&cfg, k_sweep_plane<S, T, MODE, NT>, blocks(c),
+                                  (const Chunk*)(L.sweep_chunks[dir] + off[t])));
     }
     return 0;
   }

@@ -6,10 +6,13 @@ free (admission by the case's device footprint, orion_footprint_estimate),
 builds its case (grid, metrics, initial state) on an admission thread while
 the GPU keeps running the admitted cases, and steps every admitted case on its
 own CUDA stream in quanta of graph-captured steps (orion_step_submit), so the
-work of all resident cases overlaps on the device; by default (batched) every
-resident case is stepped in one group, one launch per stage over the blocks
-of all of them (orion_group_*), rebuilt between quanta when cases join or
-retire.  A case retires at the end
+work of all resident cases overlaps on the device.  With batched=True every
+resident case is stepped in one group instead, one launch per stage over the
+blocks of all of them (orion_group_*), rebuilt between quanta when cases join
+or retire.  Streams are the default: on the C4 request mix they served about
+1.4x the group's throughput, because one case's line kernels overlap other
+cases' sweep chains, while a group's stages run one after another and its
+sweep chain is as long as its largest member's.  A case retires at the end
 of the first quantum in which its residual has dropped to `drop` times its
 first-step residual (rms, ResidualMonitor::compute), or after max_steps, or
 as diverged when its residual stops being finite or grows past diverge_growth
@@ -137,7 +140,7 @@ class Server:
     def __init__(self, precision: int = _lib.PREC_MIXED, device: int = 0, hbm_budget: Optional[int] = None,
                  max_active: int = 256, quantum: int = 20, keep_state: bool = False, builders: int = 4,
                  diverge_growth: float = 1e3, clock: Callable[[], float] = time.perf_counter,
-                 batched: bool = True):
+                 batched: bool = False):
         self.batched = batched
         self.precision = precision
         self.device = device
@@ -408,10 +411,11 @@ def main():
     ap.add_argument("--quantum", type=int, default=20)
     ap.add_argument("--max-active", type=int, default=256)
     ap.add_argument("--baseline", action="store_true", help="also serve one at a time on the plain FP64 path")
+    ap.add_argument("--group", action="store_true", help="step every resident case in one group (orion_group_*)")
     a = ap.parse_args()
     reqs = c4_requests(a.requests, a.seed, a.mean_ms, a.max_steps, a.drop)
     out = {"config": vars(a)}
-    srv = Server(_lib.PREC_MIXED, quantum=a.quantum, max_active=a.max_active)
+    srv = Server(_lib.PREC_MIXED, quantum=a.quantum, max_active=a.max_active, batched=a.group)
     out["mixed_continuous"] = summarize(srv.run(reqs))
     out["mixed_continuous"]["peak_resident_cases"] = srv.peak_resident
     if a.baseline:
