@@ -257,9 +257,12 @@ int orion_case_poll(orion_case_t c, orion_residual_t* out, int cap, int* n);
  *   orion_io_get   enqueues the copy of one block's prim as the last io step
  *                  left it into PINNED host memory, on the output copy stream;
  *   orion_io_wait  waits for every copy and step enqueued.
- * The device orders them: a put issued after an io step starts once that step
- * has installed the earlier puts, and an io step overwrites the output staging
- * only after the gets of the previous one have read it.  Results are
+ * Input and output staging are double-buffered: the puts for the next io step
+ * fill one input buffer while the current one is installed, and an io step
+ * stages its result in one output buffer while the gets of the previous step
+ * still read the other.  The device orders them: a put reuses a buffer once
+ * the io step two back has installed it, and an io step overwrites an output
+ * buffer only after the gets issued from it have read it.  Results are
  * bit-identical to upload, step, download.  Host buffers stay untouched by the
  * caller until orion_io_wait (pageable memory works but does not overlap).
  * Not for shards or grouped cases. */

@@ -133,17 +133,36 @@ struct ShardLists {
 
 // Pipelined host I/O (orion_io_*): staging copies of every block's prim and
 // the copy streams and events that order them against the steps.
+// One block's staging copy: n doubles from src to dst and, when shadow is
+// set, the same values rounded to FP32 (the mixed path's prim shadow).
+struct IoSpan {
+  const double* src;
+  double* dst;
+  float* shadow;
+  long long n;
+};
+
+// Two input and two output staging buffers, used in turn: the host copy of
+// the next input lands in one while the other is installed, and the result of
+// a step is staged in one while the host still reads the previous result
+// from the other.
 struct IoPipe {
+  IoSpan* spans_in[2] = {nullptr, nullptr};   // device: staging k -> prim (+ shadow), one per block
+  IoSpan* spans_out[2] = {nullptr, nullptr};  // device: prim -> staging k, one per block
   cudaStream_t in = nullptr, out = nullptr;
-  double* stage_in = nullptr;
-  double* stage_out = nullptr;
-  std::vector<size_t> off;     // each block's prim in the staging buffers (doubles)
+  double* stage_in[2] = {nullptr, nullptr};
+  double* stage_out[2] = {nullptr, nullptr};
+  std::vector<size_t> off;     // each block's prim in a staging buffer (doubles)
+  long long max_n = 0;         // the longest span
   std::vector<uint8_t> put;    // blocks put since the last io step
-  cudaEvent_t in_ready = nullptr, in_free = nullptr, out_ready = nullptr, out_free = nullptr;
-  bool put_waits = false;      // the next put waits for in_free (an io step installed the staging)
-  bool step_waits = false;     // the next io step waits for out_free (gets read the staging)
-  bool get_waits = false;      // the next get waits for out_ready (a new io step filled the staging)
-  bool have_out = false;
+  int put_buf = 0;             // the input buffer the next puts fill
+  int out_buf = 0;             // the output buffer the next io step fills
+  int get_buf = -1;            // the output buffer gets read (the last io step's)
+  cudaEvent_t in_ready[2] = {nullptr, nullptr}, in_free[2] = {nullptr, nullptr};
+  cudaEvent_t out_ready[2] = {nullptr, nullptr}, out_free[2] = {nullptr, nullptr};
+  bool put_waits[2] = {false, false};   // a put into buffer k waits for in_free[k] (its last install)
+  bool step_waits[2] = {false, false};  // staging into buffer k waits for out_free[k] (its last gets)
+  bool got[2] = {false, false};         // gets were issued from buffer k since it was filled
 };
 
 struct orion_case_s {
@@ -172,7 +191,6 @@ struct orion_case_s {
   long long pending_first = 0;
   int pending_n = 0;
   struct orion_group_s* group = nullptr;  // the group the case steps in, if any
-  orion::ParamsDev* d_params = nullptr;   // device copy of P, read by the kernels through the blocks
   // host copies of the work lists uploaded at set-up, by device address: a
   // group is built from them without reading the lists back
   std::unordered_map<const void*, std::vector<unsigned char>> list_mirror;

@@ -6,7 +6,13 @@ namespace orion {
 
 constexpr int NG = 3;  // ghost layers (src/preprocess/FlowField.cpp:9-16)
 
-struct ParamsDev;
+// Scalar parameters (orion_params_t after conversion).
+struct ParamsDev {
+  double gamma, moo, reynolds, prl, cfl, twall, tref, visc;
+  double roo, uoo, voo, woo, poo, too;
+  double csrv;
+  int nvis, method;
+};
 
 // One block's device arrays.  Every field is the reference's padded layout
 // (i fastest, component slowest, component stride npad).  S is the storage
@@ -59,22 +65,10 @@ struct BlockDev {
   S* sk_pair;             // 30: per face neighbour q (lower i,j,k, upper i,j,k): l1, x1, x2, ct_n, rv/2
   S* sk_gm;               // 3 (static): |grad xi|, |grad eta|, |grad zeta| of the point's metrics
   S* sk_inv;              // 3 (static): 1 / max(|grad .|, 1e-30)
-  // the parameters of the block's case (a device copy): kernels read them
-  // here, so one launch can cover the blocks of several cases (orion_group_*)
-  const ParamsDev* params;
-  // the two parameters the hyperplane sweeps read, copied here so that they
-  // arrive with the block's own fields (one dependent load fewer on the sweep
-  // chain); equal to params->gamma and params->nvis
-  double sweep_gamma;
-  int sweep_nvis;
-};
-
-// Scalar parameters (orion_params_t after conversion).
-struct ParamsDev {
-  double gamma, moo, reynolds, prl, cfl, twall, tref, visc;
-  double roo, uoo, voo, woo, poo, too;
-  double csrv;
-  int nvis, method;
+  // the parameters of the block's case: kernels read them here, with the
+  // block's other fields (no further dependent load), so one launch can
+  // cover the blocks of several cases (orion_group_*)
+  ParamsDev prm;
 };
 
 // A contiguous chunk of one block's points (padded or interior index space).

@@ -116,7 +116,7 @@ __global__ void k_bc_phase(const BlockDev<S>* __restrict__ blocks, const RegionD
   const int pt = blockIdx.x * blockDim.x + threadIdx.x;
   if (pt >= R.npts) return;
   const BlockDev<S> B = blocks[R.block];
-  const ParamsDev& P = *B.params;
+  const ParamsDev& P = B.prm;
   const int wi = R.hi[0] - R.lo[0] + 1, wj = R.hi[1] - R.lo[1] + 1;
   const int i = R.lo[0] + pt % wi;
   const int j = R.lo[1] + (pt / wi) % wj;
@@ -455,7 +455,7 @@ __global__ void k_state(const BlockDev<S>* __restrict__ blocks, const Chunk* __r
                         double* __restrict__ dt_part) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const ParamsDev& P = *B.params;
+  const ParamsDev& P = B.prm;
   double local_min = 1000.0;
 #pragma unroll 4
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
@@ -486,7 +486,7 @@ __global__ void k_timestep(const BlockDev<S>* __restrict__ blocks, const Chunk* 
                         double* __restrict__ dt_part) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const ParamsDev& P = *B.params;
+  const ParamsDev& P = B.prm;
   double local_min = 1000.0;
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
     const long long n = ch.start + t;  // interior index
@@ -692,7 +692,7 @@ __global__ void __launch_bounds__(256, LineMinBlocks<T>::visc) k_viscous(const B
   T* fsh = reinterpret_cast<T*>(smem_raw);
   const LineTile tl = tiles[blockIdx.x];
   const BlockDev<S> B = blocks[tl.block];
-  const ParamsDev& P = *B.params;
+  const ParamsDev& P = B.prm;
   const int L = dim_along(B, D);
   const int nf = L + 1;
   const long long st = stride_along(B, D);
@@ -969,7 +969,7 @@ __global__ void __launch_bounds__(256, LineMinBlocks<T>::inv) k_inviscid(const B
   T* fsh = reinterpret_cast<T*>(smem_raw);
   const LineTile tl = tiles[blockIdx.x];
   const BlockDev<S> B = blocks[tl.block];
-  const ParamsDev& P = *B.params;
+  const ParamsDev& P = B.prm;
   const int L = dim_along(B, D);
   const int nf = L + 1;
   const long long st = stride_along(B, D);
@@ -1142,7 +1142,7 @@ template <typename S, typename T, bool PAIRS = true>
 __global__ void k_lusgs_prep(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const ParamsDev& P = *B.params;
+  const ParamsDev& P = B.prm;
   const long long np = B.npad, nc = B.ncomp;
   const T gamma = T(P.gamma), reynolds = T(P.reynolds);
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
@@ -1215,7 +1215,7 @@ template <typename S, typename T>
 __global__ void k_sweep_pairs(const BlockDev<S>* __restrict__ blocks, const Chunk* __restrict__ chunks) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const ParamsDev& P = *B.params;
+  const ParamsDev& P = B.prm;
   const long long nc = B.ncomp;
   const T gamma = T(P.gamma);
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
@@ -1449,8 +1449,8 @@ __global__ void __launch_bounds__(NT, ORION_SWEEP_SM_THREADS / NT) k_sweep_plane
   // issuing loads lengthens the chain: it competes with the previous
   // hyperplane's launch, which is still running on the same SMs (forming a GS
   // pass's stale-side terms there, or even gamma - 1, made the step slower).
-  const double gamma_ld = B.sweep_gamma;
-  const int nvis = B.sweep_nvis;
+  const double gamma_ld = B.prm.gamma;
+  const int nvis = B.prm.nvis;
   const long long nc = B.ncomp;
   const int c = (int)ch.start + threadIdx.x;
   // pointers into registers now: griddepcontrol.wait clobbers memory, so
@@ -1767,15 +1767,21 @@ __device__ __forceinline__ void res_combine(double& sum, double& mx, long long& 
 template <int NT>
 __device__ __forceinline__ void block_reduce_res(double& sum, double& mx, long long& key);
 
+// CTAs per SM the finish kernel is compiled for (register cap 65536 / (NT n)):
+// on C3 four (64 registers, a few spilled) took the update stage from 7.43 to
+// 7.04 ms mixed and 11.93 to 11.54 ms plain against no cap (105 registers).
+#ifndef ORION_FINISH_MINB
+#define ORION_FINISH_MINB 4
+#endif
 template <typename S, bool DO_RES, int NT>
-__global__ void __launch_bounds__(NT) k_sweep_finish(const BlockDev<S>* __restrict__ blocks,
+__global__ void __launch_bounds__(NT, ORION_FINISH_MINB) k_sweep_finish(const BlockDev<S>* __restrict__ blocks,
                                                      const Chunk* __restrict__ chunks, ResPartial* __restrict__ partials) {
   // Natural order (interior index n = i + ni*(j + nj*k)): prim, dq, vol, dt
   // and the mask are read and written coalesced; only the swept increment is
   // gathered from the plane-major layout, at c = koff[s*nk + k] + (j - jlo(s,k)).
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const ParamsDev& P = *B.params;
+  const ParamsDev& P = B.prm;
   const long long np = B.npad, nc = B.ncomp;
   double sum = 0.0, mx = -1.0;
   long long key = (long long)0x7fffffffffffffffLL;
@@ -1910,7 +1916,7 @@ __global__ void __launch_bounds__(NT) k_update_res(const BlockDev<S>* __restrict
                                                     ResPartial* __restrict__ partials) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const ParamsDev& P = *B.params;
+  const ParamsDev& P = B.prm;
   const long long np = B.npad;
   double sum = 0.0, mx = -1.0;
   long long key = (long long)0x7fffffffffffffffLL;
@@ -2041,7 +2047,7 @@ __global__ void k_init_flow(const BlockDev<S>* __restrict__ blocks, const Chunk*
                             const long long* __restrict__ pad_base, unsigned long long seed, double amp) {
   const Chunk ch = chunks[blockIdx.x];
   const BlockDev<S> B = blocks[ch.block];
-  const ParamsDev& P = *B.params;
+  const ParamsDev& P = B.prm;
   const long long np = B.npad;
   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
     const long long idx = ch.start + t;

@@ -131,7 +131,7 @@ void carve_block(char* base, const HostBlock& b, BlockDev<S>& d) {
   d.sk_pair = sk + 44 * nc;
   d.sk_gm = sk + 74 * nc;
   d.sk_inv = sk + 77 * nc;
-  d.params = nullptr;  // set by the caller: the case's device copy of its parameters
+  d.prm = ParamsDev{};  // set by the caller: the case's parameters
   d.ni = b.idim;
   d.nj = b.jdim;
   d.nk = b.kdim;
@@ -784,17 +784,11 @@ static int create_case(int nglobal, const orion_block_desc_t* blocks, const int*
   c->arena_bytes = total;
   CUDA_TRY(cudaMemsetAsync(c->arena, 0, total, c->stream));
   std::vector<long long> prim_off(nblocks);
-  // the case's parameters in device memory: every kernel reads them through
-  // its block's descriptor (so blocks of several cases can share a launch)
-  if ((rc = dev_alloc(c.get(), &c->d_params, 1))) return rc;
-  CUDA_TRY(cudaMemcpyAsync(c->d_params, &c->P, sizeof(ParamsDev), cudaMemcpyHostToDevice, c->stream));
   if (precision == ORION_PREC_FP64) {
     c->bd64.resize(nblocks);
     for (int b = 0; b < nblocks; ++b) {
       carve_block(static_cast<char*>(c->arena) + boff[b], c->hb[b], c->bd64[b]);
-      c->bd64[b].params = c->d_params;
-      c->bd64[b].sweep_gamma = c->P.gamma;
-      c->bd64[b].sweep_nvis = c->P.nvis;
+      c->bd64[b].prm = c->P;  // every kernel reads its case's parameters from its block's descriptor
       c->bd64[b].int_base = gint[plan.local[b]];
       prim_off[b] = (c->bd64[b].prim - static_cast<double*>(c->arena));
     }
@@ -805,9 +799,7 @@ static int create_case(int nglobal, const orion_block_desc_t* blocks, const int*
     c->bd32.resize(nblocks);
     for (int b = 0; b < nblocks; ++b) {
       carve_block(static_cast<char*>(c->arena) + boff[b], c->hb[b], c->bd32[b]);
-      c->bd32[b].params = c->d_params;
-      c->bd32[b].sweep_gamma = c->P.gamma;
-      c->bd32[b].sweep_nvis = c->P.nvis;
+      c->bd32[b].prm = c->P;  // every kernel reads its case's parameters from its block's descriptor
       c->bd32[b].int_base = gint[plan.local[b]];
       prim_off[b] = (c->bd32[b].prim - static_cast<double*>(c->arena));
     }
@@ -919,10 +911,7 @@ namespace {
 
 template <typename S>
 int refresh_blocks(orion_case_t c, std::vector<BlockDev<S>>& bd) {
-  for (auto& b : bd) {
-    b.sweep_gamma = c->P.gamma;
-    b.sweep_nvis = c->P.nvis;
-  }
+  for (auto& b : bd) b.prm = c->P;
   if (bd.empty()) return 0;
   CUDA_TRY(cudaMemcpyAsync(c->d_blocks, bd.data(), sizeof(BlockDev<S>) * bd.size(), cudaMemcpyHostToDevice, c->stream));
   if (c->group) {
@@ -946,9 +935,8 @@ int orion_case_set_params(orion_case_t c, const orion_params_t* params) {
   if (!c || !params) return fail(ORION_E_INVALID, "null argument");
   std::lock_guard<std::mutex> lk(g_struct_mu);
   set_params_dev(c->P, *params);
-  // the device copy the kernels read, after the launches already enqueued
-  CUDA_TRY(cudaMemcpyAsync(c->d_params, &c->P, sizeof(ParamsDev), cudaMemcpyHostToDevice, c->stream));
-  // and the sweeps' copies in the block descriptors (the case's, and its group's)
+  // the copies in the block descriptors the kernels read (the case's, and its
+  // group's), after the launches already enqueued
   int rc = refresh_block_params(c);
   if (rc) return rc;
   CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1467,27 +1455,50 @@ int orion_case_poll(orion_case_t c, orion_residual_t* out, int cap, int* n) {
 // ---- pipelined host I/O (orion_io_*) -------------------------------------
 namespace {
 
-// Staging copies on the SMs: a cudaMemcpyAsync between device buffers would
-// queue on the copy engines behind the host copies of the neighbouring steps.
-__global__ void k_copy_doubles(const double* __restrict__ src, double* __restrict__ dst, long long n) {
+// Staging copies on the SMs, every block's in one launch (blockIdx.y is the
+// block): a cudaMemcpyAsync between device buffers would queue on the copy
+// engines behind the host copies of the neighbouring steps, and one launch
+// per block left the SMs mostly idle between small copies.  Installing an
+// input also writes the mixed path's FP32 prim shadow from the same loads
+// (the values k_prim_shadow writes).  Spans start 16-byte aligned.
+__global__ void k_io_copy(const IoSpan* __restrict__ spans) {
+  const IoSpan sp = spans[blockIdx.y];
+  const long long n2 = sp.n / 2;
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0) {
-    const long long n2 = n / 2;
-    for (long long i = t; i < n2; i += stride)
-      reinterpret_cast<double2*>(dst)[i] = reinterpret_cast<const double2*>(src)[i];
-    if (t == 0 && (n & 1)) dst[n - 1] = src[n - 1];
-  } else {
-    for (long long i = t; i < n; i += stride) dst[i] = src[i];
+  const double2* src = reinterpret_cast<const double2*>(sp.src);
+  double2* dst = reinterpret_cast<double2*>(sp.dst);
+  float2* sh = reinterpret_cast<float2*>(sp.shadow);
+  for (long long i = t; i < n2; i += stride) {
+    const double2 v = src[i];
+    dst[i] = v;
+    if (sh) sh[i] = make_float2((float)v.x, (float)v.y);
+  }
+  if (t == 0 && (sp.n & 1)) {
+    const double v = sp.src[sp.n - 1];
+    sp.dst[sp.n - 1] = v;
+    if (sp.shadow) sp.shadow[sp.n - 1] = (float)v;
   }
 }
 
-int copy_doubles(const double* src, double* dst, long long n, cudaStream_t st) {
-  const long long want = (n / 2 + 255) / 256;
-  const int grid = (int)std::max<long long>(1, std::min<long long>(want, 148LL * 8));
-  k_copy_doubles<<<grid, 256, 0, st>>>(src, dst, n);
+int io_copy(const IoSpan* spans, int nspans, long long max_n, cudaStream_t st) {
+  if (nspans <= 0) return 0;
+  const long long want = (max_n / 2 + 255) / 256;
+  const int gx = (int)std::max<long long>(1, std::min<long long>(want, std::max(1, 148 * 16 / nspans)));
+  k_io_copy<<<dim3(gx, nspans), 256, 0, st>>>(spans);
   CUDA_TRY(cudaGetLastError());
   return 0;
+}
+
+void io_free_buffers(IoPipe* io) {
+  for (int k = 0; k < 2; ++k) {
+    if (io->stage_in[k]) cudaFree(io->stage_in[k]);
+    if (io->stage_out[k]) cudaFree(io->stage_out[k]);
+    if (io->spans_in[k]) cudaFree(io->spans_in[k]);
+    if (io->spans_out[k]) cudaFree(io->spans_out[k]);
+    io->stage_in[k] = io->stage_out[k] = nullptr;
+    io->spans_in[k] = io->spans_out[k] = nullptr;
+  }
 }
 
 int io_pipe(orion_case_t c, IoPipe** out) {
@@ -1504,17 +1515,37 @@ int io_pipe(orion_case_t c, IoPipe** out) {
     total += ((size_t)c->hb[b].npad * 6 + 1) / 2 * 2;  // 16-byte aligned starts
   }
   io->put.assign(c->nblocks, 0);
-  auto cleanup = [&](const char* what) {
-    if (io->stage_in) cudaFree(io->stage_in);
-    if (io->stage_out) cudaFree(io->stage_out);
-    return fail(ORION_E_NOMEM, what);
-  };
-  if (cudaMalloc((void**)&io->stage_in, total * sizeof(double)) != cudaSuccess) return cleanup("input staging");
-  if (cudaMalloc((void**)&io->stage_out, total * sizeof(double)) != cudaSuccess) return cleanup("output staging");
+  std::vector<void*> prim(c->nblocks);
+  for (int b = 0; b < c->nblocks; ++b) {
+    int nc;
+    bool st;
+    int rc = field_info(c, b, ORION_FIELD_PRIM, &prim[b], &nc, &st);
+    if (rc) return rc;
+    io->max_n = std::max(io->max_n, 6 * (long long)c->hb[b].npad);
+  }
+  for (int k = 0; k < 2; ++k) {
+    if (cudaMalloc((void**)&io->stage_in[k], total * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void**)&io->stage_out[k], total * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void**)&io->spans_in[k], sizeof(IoSpan) * c->nblocks) != cudaSuccess ||
+        cudaMalloc((void**)&io->spans_out[k], sizeof(IoSpan) * c->nblocks) != cudaSuccess) {
+      cudaGetLastError();
+      io_free_buffers(io.get());
+      return fail(ORION_E_NOMEM, "pipelined I/O staging");
+    }
+    std::vector<IoSpan> sin(c->nblocks), sout(c->nblocks);
+    for (int b = 0; b < c->nblocks; ++b) {
+      const long long n = 6 * (long long)c->hb[b].npad;
+      float* sh = c->prec == ORION_PREC_FP64 ? nullptr : c->bd32[b].prim_f;
+      sin[b] = IoSpan{io->stage_in[k] + io->off[b], static_cast<double*>(prim[b]), sh, n};
+      sout[b] = IoSpan{static_cast<const double*>(prim[b]), io->stage_out[k] + io->off[b], nullptr, n};
+    }
+    CUDA_TRY(cudaMemcpy(io->spans_in[k], sin.data(), sizeof(IoSpan) * c->nblocks, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(io->spans_out[k], sout.data(), sizeof(IoSpan) * c->nblocks, cudaMemcpyHostToDevice));
+    for (cudaEvent_t* e : {&io->in_ready[k], &io->in_free[k], &io->out_ready[k], &io->out_free[k]})
+      CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  }
   CUDA_TRY(cudaStreamCreateWithFlags(&io->in, cudaStreamNonBlocking));
   CUDA_TRY(cudaStreamCreateWithFlags(&io->out, cudaStreamNonBlocking));
-  for (cudaEvent_t* e : {&io->in_ready, &io->in_free, &io->out_ready, &io->out_free})
-    CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   c->io = io.release();
   *out = c->io;
   return 0;
@@ -1526,10 +1557,10 @@ void io_release(orion_case_t c) {
   if (io->in) cudaStreamSynchronize(io->in);
   if (io->out) cudaStreamSynchronize(io->out);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  cudaFree(io->stage_in);
-  cudaFree(io->stage_out);
-  for (cudaEvent_t e : {io->in_ready, io->in_free, io->out_ready, io->out_free})
-    if (e) cudaEventDestroy(e);
+  io_free_buffers(io);
+  for (int k = 0; k < 2; ++k)
+    for (cudaEvent_t e : {io->in_ready[k], io->in_free[k], io->out_ready[k], io->out_free[k]})
+      if (e) cudaEventDestroy(e);
   if (io->in) cudaStreamDestroy(io->in);
   if (io->out) cudaStreamDestroy(io->out);
   delete io;
@@ -1555,11 +1586,12 @@ int orion_io_put(orion_case_t c, int block, const double* host) {
   IoPipe* io = nullptr;
   int rc = io_pipe(c, &io);
   if (rc) return rc;
-  if (io->put_waits) {  // the last io step must have installed the staging first
-    CUDA_TRY(cudaStreamWaitEvent(io->in, io->in_free, 0));
-    io->put_waits = false;
+  const int k = io->put_buf;
+  if (io->put_waits[k]) {  // the io step that installed this buffer last must be done with it
+    CUDA_TRY(cudaStreamWaitEvent(io->in, io->in_free[k], 0));
+    io->put_waits[k] = false;
   }
-  CUDA_TRY(cudaMemcpyAsync(io->stage_in + io->off[block], host, sizeof(double) * 6 * (size_t)c->hb[block].npad,
+  CUDA_TRY(cudaMemcpyAsync(io->stage_in[k] + io->off[block], host, sizeof(double) * 6 * (size_t)c->hb[block].npad,
                            cudaMemcpyHostToDevice, io->in));
   io->put[block] = 1;
   return 0;
@@ -1572,27 +1604,27 @@ int orion_io_step(orion_case_t c, int nsteps) {
   if (rc) return rc;
   if (c->pending_n + nsteps > kHistCap)
     return fail(ORION_E_INVALID, "more unpolled steps than the history ring holds (4096)");
-  // install the blocks put since the last io step
+  // install the blocks put since the last io step, from the input buffer they filled
   bool any = false;
   for (int b = 0; b < c->nblocks; ++b) any = any || io->put[b];
   if (any) {
-    CUDA_TRY(cudaEventRecord(io->in_ready, io->in));
-    CUDA_TRY(cudaStreamWaitEvent(c->stream, io->in_ready, 0));
-    for (int b = 0; b < c->nblocks; ++b) {
-      if (!io->put[b]) continue;
-      void* d;
-      int nc;
-      bool st;
-      if ((rc = field_info(c, b, ORION_FIELD_PRIM, &d, &nc, &st))) return rc;
-      if ((rc = copy_doubles(io->stage_in + io->off[b], static_cast<double*>(d), 6 * (long long)c->hb[b].npad,
-                             c->stream)))
-        return rc;
-      rc = dispatch(c, [&](const StageOps& o) { return o.prim_shadow(c, b); });
-      if (rc) return rc;
-      io->put[b] = 0;
+    const int k = io->put_buf;
+    CUDA_TRY(cudaEventRecord(io->in_ready[k], io->in));
+    CUDA_TRY(cudaStreamWaitEvent(c->stream, io->in_ready[k], 0));
+    // runs of consecutive put blocks, one launch each (one launch when all were put)
+    for (int b = 0; b < c->nblocks;) {
+      if (!io->put[b]) {
+        ++b;
+        continue;
+      }
+      int e = b;
+      while (e < c->nblocks && io->put[e]) io->put[e++] = 0;
+      if ((rc = io_copy(io->spans_in[k] + b, e - b, io->max_n, c->stream))) return rc;
+      b = e;
     }
-    CUDA_TRY(cudaEventRecord(io->in_free, c->stream));
-    io->put_waits = true;
+    CUDA_TRY(cudaEventRecord(io->in_free[k], c->stream));
+    io->put_waits[k] = true;
+    io->put_buf = k ^ 1;  // the next puts fill the other buffer while this step runs
   }
   if (!c->hist_host && !(c->hist_host = acquire_hist_ring())) return fail(ORION_E_NOMEM, "pinned history ring");
   if (c->hist_count < 0) {  // once: learn the device counter
@@ -1602,43 +1634,38 @@ int orion_io_step(orion_case_t c, int nsteps) {
     c->hist_count = cnt;
   }
   if (nsteps > 0 && (rc = launch_steps(c, nsteps))) return rc;
-  // the result into the output staging, once the previous gets have read it
-  if (io->step_waits) {
-    CUDA_TRY(cudaEventRecord(io->out_free, io->out));
-    CUDA_TRY(cudaStreamWaitEvent(c->stream, io->out_free, 0));
-    io->step_waits = false;
+  // the gets issued so far from the last filled buffer end where out_free says
+  if (io->get_buf >= 0 && io->got[io->get_buf]) {
+    CUDA_TRY(cudaEventRecord(io->out_free[io->get_buf], io->out));
+    io->step_waits[io->get_buf] = true;
+    io->got[io->get_buf] = false;
   }
-  for (int b = 0; b < c->nblocks; ++b) {
-    void* d;
-    int nc;
-    bool st;
-    if ((rc = field_info(c, b, ORION_FIELD_PRIM, &d, &nc, &st))) return rc;
-    if ((rc = copy_doubles(static_cast<const double*>(d), io->stage_out + io->off[b], 6 * (long long)c->hb[b].npad,
-                           c->stream)))
-      return rc;
+  // the result into the other output buffer, once its own last gets have read it
+  const int j = io->out_buf;
+  if (io->step_waits[j]) {
+    CUDA_TRY(cudaStreamWaitEvent(c->stream, io->out_free[j], 0));
+    io->step_waits[j] = false;
   }
-  CUDA_TRY(cudaEventRecord(io->out_ready, c->stream));
+  if ((rc = io_copy(io->spans_out[j], c->nblocks, io->max_n, c->stream))) return rc;
+  CUDA_TRY(cudaEventRecord(io->out_ready[j], c->stream));
   // the residual history leaves with the state, on the output copy stream: on
   // the case's stream that small copy would queue on the copy engine behind
   // the previous state's copy to the host and hold up the next step
-  CUDA_TRY(cudaStreamWaitEvent(io->out, io->out_ready, 0));
+  CUDA_TRY(cudaStreamWaitEvent(io->out, io->out_ready[j], 0));
   if (nsteps > 0 && (rc = enqueue_hist_copy(c, nsteps, io->out))) return rc;
-  io->get_waits = false;
-  io->have_out = true;
+  io->get_buf = j;
+  io->out_buf = j ^ 1;
   return 0;
 }
 
 int orion_io_get(orion_case_t c, int block, double* host) {
   if (!c || !host || block < 0 || block >= c->nblocks) return fail(ORION_E_INVALID, "bad arguments");
   IoPipe* io = c->io;
-  if (!io || !io->have_out) return fail(ORION_E_INVALID, "no io step has run");
-  if (io->get_waits) {
-    CUDA_TRY(cudaStreamWaitEvent(io->out, io->out_ready, 0));
-    io->get_waits = false;
-  }
-  CUDA_TRY(cudaMemcpyAsync(host, io->stage_out + io->off[block], sizeof(double) * 6 * (size_t)c->hb[block].npad,
+  if (!io || io->get_buf < 0) return fail(ORION_E_INVALID, "no io step has run");
+  const int j = io->get_buf;  // the output stream already waits for this buffer's staging
+  CUDA_TRY(cudaMemcpyAsync(host, io->stage_out[j] + io->off[block], sizeof(double) * 6 * (size_t)c->hb[block].npad,
                            cudaMemcpyDeviceToHost, io->out));
-  io->step_waits = true;
+  io->got[j] = true;
   return 0;
 }
 

@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(32 * TileShape<T>::TK + 32) k_sweep_tiles(cons
   if (slot >= ntiles) return;
   const SweepTile W = tiles[slot];
   const BlockDev<S>& Bd = blocks[W.block];
-  const ParamsDev& P = *Bd.params;
+  const ParamsDev& P = Bd.prm;
   const int ni = Bd.ni;
   const int nsteps = ni + TJ + TK - 2;
 
