@@ -684,9 +684,11 @@ __device__ __forceinline__ void tile_item(int it, int nlanes, int nfaces, int& l
 }
 
 // CTAs per SM the line kernels are compiled for (register cap 65536/(256*n)),
-// per compute precision, measured on C3: FP32 six (viscous) and five (inviscid), FP64 three and two.
+// per compute precision, measured on C3: FP32 five (viscous; 3.91 ms against
+// 4.03 at six and 4.09 at four) and five (inviscid; four and six were slower),
+// FP64 three and two.
 #ifndef ORION_VISC_MINB_F32
-#define ORION_VISC_MINB_F32 6
+#define ORION_VISC_MINB_F32 5
 #endif
 #ifndef ORION_INV_MINB_F32
 #define ORION_INV_MINB_F32 5
