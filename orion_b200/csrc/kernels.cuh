@@ -980,6 +980,46 @@ __device__ void cascade_right(const BlockDev<S>& B, const InvLine<S, T>& ln, int
   for (int m = 0; m < 5; ++m) fc[m] = -cs.acc[m] / T(24.0);
 }
 
+// Boundary re-calculation of flagged line ends (InviscidFluxComputer.cpp:377-521)
+// for one tile: the six outputs of each line's two ends by consecutive threads.
+// k_inviscid's regular loop skips these points, so each point's dq gets
+// direction D's terms once and in direction order.
+template <int D, typename S, typename T>
+__device__ __forceinline__ void inv_boundary_rounds(const BlockDev<S>& B, const LineTile& tl, int L, long long st,
+                                                    T gamma) {
+  const int nbnd = tl.count * 6;
+  for (int it = threadIdx.x; it < nbnd; it += blockDim.x) {
+    const int lane = it / 6, slot = it - lane * 6;
+    const long long o = line_origin(B, D, tl.first + lane);
+    const bool left = slot < 3;
+    const bool flag = left ? (B.prim[o] < 1.0e-20) : (B.prim[o + (long long)(L + 5) * st] < 1.0e-20);
+    if (!flag) continue;
+    const int t = left ? slot : L - 6 + slot;
+    InvLine<S, T> ln{FluxSrc<S>::prim(B), o, st, B.npad, L};
+    T fc[5];
+    if (left) cascade_left<D, S, T>(B, ln, t, gamma, fc);
+    else cascade_right<D, S, T>(B, ln, t, gamma, fc);
+    const long long idx = o + (long long)(t + NG) * st;
+    for (int m = 0; m < 5; ++m) {
+      S* q = B.dq + m * B.npad + idx;
+      *q = (S)((T)*q + fc[m]);
+    }
+  }
+}
+
+// The FP32 path runs the boundary rounds in their own launch after
+// k_inviscid<D>, over the same tiles: inlined, their Roe fluxes need about 128
+// registers, against 48 for the face loop (3.53 against 3.61 ms on C3).  The
+// FP64 path keeps them in k_inviscid: its face loop is bound by the FP64 pipe,
+// and the extra launch cost it 0.4 ms.
+template <int D, typename S, typename T>
+__global__ void __launch_bounds__(256) k_inv_cascade(const BlockDev<S>* __restrict__ blocks,
+                                                     const LineTile* __restrict__ tiles) {
+  const LineTile tl = tiles[blockIdx.x];
+  const BlockDev<S> B = blocks[tl.block];
+  inv_boundary_rounds<D, S, T>(B, tl, dim_along(B, D), stride_along(B, D), T(B.prm.gamma));
+}
+
 template <int D, typename S, typename T>
 __global__ void __launch_bounds__(256, LineMinBlocks<T>::inv) k_inviscid(const BlockDev<S>* __restrict__ blocks, const LineTile* __restrict__ tiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1023,27 +1063,10 @@ __global__ void __launch_bounds__(256, LineMinBlocks<T>::inv) k_inviscid(const B
       *q = (S)((T)*q + flux_diff<T>(fb + m, 5, t, L));
     }
   }
-  // boundary re-calculation of flagged line ends, six outputs per line handled
-  // by consecutive threads so the rounds do not stall the regular warps
-  const int nbnd = tl.count * 6;
-  for (int it = threadIdx.x; it < nbnd; it += blockDim.x) {
-    const int lane = it / 6, slot = it - lane * 6;
-    const long long o = line_origin(B, D, tl.first + lane);
-    const bool left = slot < 3;
-    const bool flag = left ? (B.prim[o] < 1.0e-20) : (B.prim[o + (long long)(L + 5) * st] < 1.0e-20);
-    if (!flag) continue;
-    const int t = left ? slot : L - 6 + slot;
-    InvLine<S, T> ln{FluxSrc<S>::prim(B), o, st, B.npad, L};
-    T fc[5];
-    if (left) cascade_left<D, S, T>(B, ln, t, gamma, fc);
-    else cascade_right<D, S, T>(B, ln, t, gamma, fc);
-    const long long idx = o + (long long)(t + NG) * st;
-    for (int m = 0; m < 5; ++m) {
-      S* q = B.dq + m * B.npad + idx;
-      *q = (S)((T)*q + fc[m]);
-    }
-  }
+
+  if constexpr (sizeof(T) == 8) inv_boundary_rounds<D, S, T>(B, tl, L, st, gamma);
 }
+
 
 // ===========================================================================
 // Interface residual averaging (HaloExchanger::average_interface_residuals,

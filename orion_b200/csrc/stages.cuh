@@ -122,6 +122,8 @@ struct Stages {
     auto& L = c->L;
     const size_t smem = (size_t)L.line_units[D] * 5 * sizeof(T);
     k_inviscid<D, S, T><<<L.n_tiles[D], kThreads, smem, c->stream>>>(blocks(c), L.tiles[D]);
+    if constexpr (sizeof(T) == 4)  // FP64: inside k_inviscid
+      k_inv_cascade<D, S, T><<<L.n_tiles[D], kThreads, 0, c->stream>>>(blocks(c), L.tiles[D]);
   }
 
   static int inviscid(orion_case_t c) {
