@@ -147,6 +147,9 @@ int validate_blocks(int nblocks, const orion_block_desc_t* blocks) {
     const auto& d = blocks[b];
     if (d.idim < 12 || d.jdim < 12 || d.kdim < 12)
       return fail(ORION_E_UNSUPPORTED, "block " + std::to_string(b) + ": every extent must be >= 12 points");
+    // interior point indices within a block are 32-bit in several kernels
+    if ((long long)(d.idim + 2 * NG) * (d.jdim + 2 * NG) * (d.kdim + 2 * NG) >= (1LL << 31))
+      return fail(ORION_E_UNSUPPORTED, "block " + std::to_string(b) + ": more than 2^31 padded points");
     if (d.nregions < 0 || (d.nregions > 0 && !d.regions))
       return fail(ORION_E_INVALID, "block " + std::to_string(b) + ": bad region list");
     for (int r = 0; r < d.nregions; ++r) {
