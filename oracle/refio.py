@@ -22,17 +22,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def ref_root() -> str:
-    """The reference's source tree (read-only): $ORION_REF, else the default
-    that oracle/Makefile (the recipe compiling it) names.  Only CPU-side checks
-    read it directly; the GPU box has no source tree."""
+    """The reference's source tree (read-only): $ORION_REF, else a directory
+    `reference` beside the repository, the default of oracle/Makefile (the
+    recipe compiling it).  Only CPU-side checks read it directly; a machine
+    without the source tree (a GPU box) uses the prebuilt oracle/_ref."""
     env = os.environ.get("ORION_REF")
     if env:
         return env
-    with open(os.path.join(HERE, "Makefile")) as f:
-        for line in f:
-            if line.startswith("ORION_REF") and "?=" in line:
-                return line.split("?=", 1)[1].strip()
-    return ""
+    return os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
 
 
 REF_ROOT = ref_root()
