@@ -73,3 +73,38 @@ def test_io_needs_a_step_before_a_get_and_refuses_grouped_cases():
     g.close()
     other.close()
     fs.close()
+
+
+def test_partial_puts_install_only_the_blocks_put():
+    """Blocks put in scattered runs (0, 2-3, 5 of 12) are installed; the others keep
+    the state the previous io step left, as with blocking uploads of those blocks."""
+    precision = _lib.PREC_MIXED
+    states = _states(precision, 2)
+    put_blocks = [0, 2, 3, 5]
+    fs = solver.FlowFieldSet(cases.small_case(**SPEC), precision=precision)
+    for b, a in enumerate(states[0]):
+        fs.upload(b, "prim", a)
+    fs.step(1)
+    for b in put_blocks:
+        fs.upload(b, "prim", states[1][b])
+    want_h = fs.step(2)
+    want = [fs.download(b, "prim") for b in range(len(states[0]))]
+    fs.close()
+    fs = solver.FlowFieldSet(cases.small_case(**SPEC), precision=precision)
+    ins0 = [torch.from_numpy(a.reshape(-1)).pin_memory() for a in states[0]]
+    ins1 = {b: torch.from_numpy(states[1][b].reshape(-1)).pin_memory() for b in put_blocks}
+    outs = [torch.empty_like(t).pin_memory() for t in ins0]
+    for b, t in enumerate(ins0):
+        fs.io_put(b, t)
+    fs.io_step(1)
+    for b in put_blocks:
+        fs.io_put(b, ins1[b])
+    fs.io_step(2)
+    for b, t in enumerate(outs):
+        fs.io_get(b, t)
+    fs.io_wait()
+    hist = fs.poll()
+    fs.close()
+    assert np.array_equal(hist[1:], want_h)
+    for b in range(len(states[0])):
+        assert np.array_equal(outs[b].numpy(), want[b].reshape(-1)), f"block {b}"
