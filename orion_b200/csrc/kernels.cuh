@@ -686,7 +686,8 @@ __device__ __forceinline__ void tile_item(int it, int nlanes, int nfaces, int& l
 // CTAs per SM the line kernels are compiled for (register cap 65536/(256*n)),
 // per compute precision, measured on C3: FP32 five (viscous; 3.91 ms against
 // 4.03 at six and 4.09 at four) and five (inviscid; four and six were slower),
-// FP64 three and two.
+// FP64 three (viscous) and three (inviscid, with its boundary rounds in their
+// own kernel; two CTAs when they were inline).
 #ifndef ORION_VISC_MINB_F32
 #define ORION_VISC_MINB_F32 5
 #endif
@@ -697,7 +698,7 @@ __device__ __forceinline__ void tile_item(int it, int nlanes, int nfaces, int& l
 #define ORION_VISC_MINB_F64 3
 #endif
 #ifndef ORION_INV_MINB_F64
-#define ORION_INV_MINB_F64 2
+#define ORION_INV_MINB_F64 3
 #endif
 template <typename T> struct LineMinBlocks;
 template <> struct LineMinBlocks<float> { static constexpr int visc = ORION_VISC_MINB_F32, inv = ORION_INV_MINB_F32; };
@@ -1007,11 +1008,12 @@ __device__ __forceinline__ void inv_boundary_rounds(const BlockDev<S>& B, const 
   }
 }
 
-// The FP32 path runs the boundary rounds in their own launch after
-// k_inviscid<D>, over the same tiles: inlined, their Roe fluxes need about 128
-// registers, against 48 for the face loop (3.53 against 3.61 ms on C3).  The
-// FP64 path keeps them in k_inviscid: its face loop is bound by the FP64 pipe,
-// and the extra launch cost it 0.4 ms.
+// The boundary rounds run in their own launch after k_inviscid<D>, over the
+// same tiles, with CTAs sized to a tile's six outputs per line: inlined, their
+// Roe fluxes need about 128 (FP32) or 250 (FP64) registers, against 48 and 80
+// for the face loop.  On C3 the split took the inviscid stage from 3.61 to
+// 3.25 ms mixed and from 12.2 to 11.9 ms plain (the FP64 face loop at three
+// CTAs per SM).
 template <int D, typename S, typename T>
 __global__ void __launch_bounds__(256) k_inv_cascade(const BlockDev<S>* __restrict__ blocks,
                                                      const LineTile* __restrict__ tiles) {
@@ -1064,7 +1066,6 @@ __global__ void __launch_bounds__(256, LineMinBlocks<T>::inv) k_inviscid(const B
     }
   }
 
-  if constexpr (sizeof(T) == 8) inv_boundary_rounds<D, S, T>(B, tl, L, st, gamma);
 }
 
 

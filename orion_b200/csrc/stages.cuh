@@ -122,7 +122,7 @@ struct Stages {
     auto& L = c->L;
     const size_t smem = (size_t)L.line_units[D] * 5 * sizeof(T);
     k_inviscid<D, S, T><<<L.n_tiles[D], kThreads, smem, c->stream>>>(blocks(c), L.tiles[D]);
-    if constexpr (sizeof(T) == 4) {  // FP64: inside k_inviscid
+    {
       // six outputs per line of the tile, whole warps: a CTA of 256 threads
       // would leave most of its registers idle (about 128 per thread)
       const int nt = std::min(kThreads, (6 * std::max(L.lanes[D], 1) + 31) / 32 * 32);
