@@ -237,7 +237,9 @@ class FlowFieldSet:
 
     def poll(self, cap: int = 4096):
         """None while submitted steps run; else their history (n, 8) as step() returns it."""
-        buf = (_lib.Residual * max(cap, 1))()
+        buf = getattr(self, "_poll_buf", None)
+        if buf is None or len(buf) < max(cap, 1):  # one buffer per case, reused: request loops poll often
+            buf = self._poll_buf = (_lib.Residual * max(cap, 1))()
         n = C.c_int()
         rc = _lib.load().orion_case_poll(self._h, buf, cap, C.byref(n))
         if rc == 0:
